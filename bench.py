@@ -1,0 +1,305 @@
+"""Gibbs-sweep benchmark of libGPUPolyaUrnLDA.so (one JSON line on rank 0).
+
+A step is one full Gibbs iteration over the whole corpus: the Phi step
+(Poisson draws, normalisers, alias tables) and one z sweep that resamples
+every token and rebuilds the counts.  Default workload: the mid configuration
+(K=1000, V=100000, D=300000, ~1.0e8 tokens; synthetic, seeded).
+
+  value   tokens/s with the corpus resident in HBM (gpulda_corpus_sweep),
+          device time from CUDA events on the library's stream, max over ranks
+  e2e     tokens/s through the reference protocol (initialize / sample_phi /
+          sample_z_async / sync_buffer) with pinned host buffers: every step
+          copies z, w, d, K_d to the device and z back
+  roofline  the z-sweep kernel's algorithmic bytes (24 N + 8 D + 4 S, S the
+          sparse work counted by the kernel) over its CUDA-event time,
+          against the measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle (same algorithm) on a bounded sample, all cores
+
+--impl reference times the CPU oracle alone (the reference has no CPU
+implementation of the path and its CUDA kernels are not run).
+Multi-GPU (torchrun): independent chains per GPU (replicas), weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "gibbs_tokens_per_sec"
+UNIT = "tokens/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="mid")
+    p.add_argument("--docs", type=int, default=None, help="override the number of documents")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the baseline sample")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_corpus(args, device):
+    from gpupolyaurnlda_b200 import corpus
+    return corpus.generate(args.workload, seed=1, device=device, D=args.docs)
+
+
+def workload_desc(c, args):
+    return {"workload": f"{args.workload}: K={c.K} V={c.V} D={c.n_docs} N={c.n_tokens} tokens "
+                        f"(synthetic LDA corpus, seed 1; random initial topics)",
+            "K": c.K, "V": c.V, "D": c.n_docs, "N": c.n_tokens, "alpha": c.alpha, "beta": c.beta,
+            "l2": "inputs larger than L2 (fixed-point Phi 4KV B, alias tables 8KV B, corpus 8N B)"}
+
+
+def cpu_baseline(c, seconds: float, threads: int | None = None):
+    """One Phi step over all K*V cells plus a z sweep over a leading slice of the
+    documents sized for ~`seconds` of work, extrapolated to a full iteration."""
+    import oracle
+    threads = threads or oracle.default_threads()
+    ch = oracle.Chain(c.K, c.alpha, c.beta, c.counts, seed=0, threads=threads)
+    t0 = time.perf_counter()
+    ch.sample_phi()
+    t_phi = time.perf_counter() - t0
+    # probe speed on a small slice, then size the sample
+    cum = np.cumsum(c.d_len.astype(np.int64))
+    probe_docs = int(np.searchsorted(cum, min(c.n_tokens, 200000))) + 1
+    probe_docs = min(probe_docs, c.n_docs)
+    ntok = int(cum[probe_docs - 1])
+    z = c.z[:ntok].copy()
+    t0 = time.perf_counter()
+    ch.sweep(c.w[:ntok], z, c.d_len[:probe_docs])
+    rate = ntok / max(1e-9, time.perf_counter() - t0)
+    want = int(min(c.n_tokens, max(ntok, rate * max(1.0, seconds - t_phi))))
+    docs = min(c.n_docs, int(np.searchsorted(cum, want)) + 1)
+    ntok = int(cum[docs - 1])
+    z = c.z[:ntok].copy()
+    ch.tok_base = 0
+    t0 = time.perf_counter()
+    ch.sweep(c.w[:ntok], z, c.d_len[:docs])
+    t_z = time.perf_counter() - t0
+    t_iter = t_phi + t_z * (c.n_tokens / ntok)
+    return {"value": c.n_tokens / t_iter, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"one Phi step over all {c.K}x{c.V} cells ({t_phi:.2f} s) + z sweep over the first {docs} "
+                      f"documents ({ntok} tokens, {t_z:.2f} s), extrapolated to {c.n_tokens} tokens"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    dev = "cuda" if _cuda() else "cpu"
+    c = make_corpus(args, dev)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(c, args.cpu_seconds)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = float(np.median(vals))
+    ms = c.n_tokens / v * 1e3
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
+            "config": dict(workload_desc(c, args), parallelism="cpu"),
+            "cpu_baseline": dict(r, value=v),
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "CPU oracle port of the sweep (the reference has no CPU implementation; its CUDA kernels are "
+                    "not run on this pool)"}
+    print(json.dumps(line), flush=True)
+
+
+def _cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import gpupolyaurnlda_b200 as g
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    c = make_corpus(args, f"cuda:{local}")
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    hbm, peak_kind = peaks()
+
+    # ---- device-resident corpus: value + roofline ----------------------------
+    s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=0, chain=rank)
+    s.set_stream(stream.cuda_stream)
+    s.corpus_load(c.z.copy(), c.w, c.d_len)
+    for _ in range(args.warmup):
+        s.corpus_sweep(1)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    z_ms, phi_ms, S_work, launches = [], [], [], 0
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.corpus_sweep(1)  # host-synchronous; events below bracket all steps
+        kt = s.kernel_times()
+        cnt = s.counters()
+        z_ms.append(kt["z_sweep"])
+        phi_ms.append(kt["phi_draw"] + kt["alias_build"] + kt["prep"])
+        S_work.append(cnt["sparse_work"])
+        launches += cnt["launches"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    s.set_stream(0)
+    s.close()
+
+    value = world * c.n_tokens * args.steps / (ms_max / 1e3)
+    zb = [24 * c.n_tokens + 8 * c.n_docs + 4 * S for S in S_work]
+    z_gbs = float(np.mean([b / (m / 1e3) / 1e9 for b, m in zip(zb, z_ms)]))
+    B_iter = [20 * c.K * c.V + b for b in zb]
+    it_gbs = float(np.mean([b / (ms_max / args.steps / 1e3) / 1e9 for b in B_iter]))
+
+    # ---- reference protocol with pinned host buffers: e2e --------------------
+    e2e = None
+    if not args.no_e2e:
+        zp = torch.from_numpy(c.z.copy()).pin_memory()
+        wp = torch.from_numpy(c.w).pin_memory()
+        dp = torch.from_numpy(c.d_len).pin_memory()
+        kp = torch.from_numpy(c.k_d()).pin_memory()
+        zn, wn, dn, kn = zp.numpy(), wp.numpy(), dp.numpy(), kp.numpy()
+        s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=c.n_tokens, max_D=c.n_docs, seed=0, chain=rank)
+        for _ in range(args.warmup):
+            s.sample_phi()
+            s.sweep_buffer(0, zn, wn, dn, kn)
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            s.sample_phi()
+            s.sweep_buffer(0, zn, wn, dn, kn)
+        el = time.perf_counter() - t0
+        s.close()
+        te = torch.tensor([el], dtype=torch.float64, device=f"cuda:{local}")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * c.n_tokens * args.steps / float(te.item()), "unit": UNIT,
+               "h2d_bytes_per_step": 8 * c.n_tokens + 8 * c.n_docs, "d2h_bytes_per_step": 4 * c.n_tokens,
+               "path": "initialize/sample_phi/sample_z_async/sync_buffer, one buffer per iteration, pinned host"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(c, args.cpu_seconds)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": dict(workload_desc(c, args),
+                               parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+                "roofline": {"bound": "hbm", "achieved": z_gbs, "peak": hbm, "unit": "GB/s",
+                             "frac": z_gbs / hbm, "traffic": None, "kernel": "z_sweep_kernel",
+                             "algorithmic_bytes_per_launch": float(np.mean(zb)), "peak_kind": peak_kind},
+                "iteration_roofline": {"achieved": it_gbs, "frac": it_gbs / hbm,
+                                       "bytes_per_iteration": float(np.mean(B_iter))},
+                "kernel_ms": {"z_sweep": float(np.mean(z_ms)), "phi_step": float(np.mean(phi_ms))},
+                "sparse_work_per_token": float(np.mean(S_work)) / c.n_tokens,
+                "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

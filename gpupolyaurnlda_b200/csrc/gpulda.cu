@@ -1,0 +1,628 @@
+// gpulda.cu -- the C ABI of libGPUPolyaUrnLDA.so (declared in include/gpulda.h).
+//
+// Device orchestration for one model per process (reference: the globals and
+// entry points of src/cu/train.cu:16-177).  The reference keeps cuBLAS,
+// cuRAND states and V separately allocated alias tables; this library keeps
+// four contiguous word-major V*K arrays (counts, fixed-point Phi, alias
+// entries) plus per-word and per-topic vectors, and no generator state.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/gpulda.h"
+#include "kernels.cuh"
+#include "tables.h"
+
+using namespace gpulda;
+
+static_assert(sizeof(Args) == 32, "Args must match src/ffi.rs Args_FFI");
+static_assert(offsetof(Args, C) == 16, "Args.C offset");
+static_assert(offsetof(Args, buffer_size) == 24, "Args.buffer_size offset");
+static_assert(sizeof(Buffer) == 96, "Buffer must match src/buffer.rs");
+static_assert(offsetof(Buffer, n_docs) == 32, "Buffer.n_docs offset");
+static_assert(offsetof(Buffer, gpu_z) == 40, "Buffer.gpu_z offset");
+static_assert(offsetof(Buffer, stream) == 88, "Buffer.stream offset");
+
+namespace {
+
+enum TimerSlot { kTPhi = 0, kTPrep = 1, kTAlias = 2, kTOffsets = 3, kTZ = 4, kTN = 5 };
+
+struct BufCtx {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  bool used = false;
+};
+
+struct Model {
+  bool live = false;
+  int fatal = 1;
+  int last_error = GPULDA_OK;
+
+  u32 K = 0, V = 0, buffer_size = 0, max_D = 0;
+  float alpha = 0, beta = 0;
+  u32 key0 = 0, key1 = 0, flags = 0;
+  int t = -1;           // current iteration (sample_phi calls - 1)
+  u64 tok_offset = 0;   // tokens swept so far in the current iteration
+  bool swept = false;   // a sweep ran since the last sample_phi
+
+  ModelDev dev{};
+  u32* C = nullptr;
+  u32* cdf = nullptr;
+  uint8_t* guide = nullptr;
+  double* lfac = nullptr;
+  unsigned long long* counters = nullptr;  // kCtrN
+  double* ll = nullptr;                     // 2
+  u32* work = nullptr;
+  u32* status = nullptr;
+  void* alias_scratch = nullptr;
+  size_t alias_scratch_bytes = 0;
+
+  cudaStream_t stream = nullptr;       // library stream
+  cudaStream_t user_stream = nullptr;  // caller-supplied stream, if any
+  cudaEvent_t ev[6] = {};
+  bool phi_timed = false, z_timed = false;
+  cudaEvent_t z_ev[3] = {};
+  u32 launches = 0;
+
+  // device-resident corpus
+  u32 *cz = nullptr, *cw = nullptr, *cd_len = nullptr, *cd_idx = nullptr, *cK_d = nullptr;
+  u32 c_docs = 0;
+  u64 c_tokens = 0;
+};
+
+Model g;
+
+const char* kErrNames[] = {"ok",
+                           "CUDA runtime error",
+                           "invalid model arguments",
+                           "call out of protocol order",
+                           "buffer exceeds buffer_size / max_D or is malformed",
+                           "device allocation failed",
+                           "a kernel reported a violated invariant",
+                           "size not supported by this build"};
+
+int fail(int code, const char* what) {
+  g.last_error = code;
+  if (g.fatal) {
+    fprintf(stderr, "GPUPolyaUrnLDA error %d (%s): %s\n", code, kErrNames[code], what);
+    exit(code);
+  }
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  char buf[256];
+  snprintf(buf, sizeof buf, "%s: %s", where, cudaGetErrorString(e));
+  return fail(e == cudaErrorMemoryAllocation ? GPULDA_ERR_NOMEM : GPULDA_ERR_CUDA, buf);
+}
+
+#define CK(expr)                                           \
+  do {                                                     \
+    cudaError_t e_ = (expr);                               \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #expr);    \
+  } while (0)
+
+cudaStream_t main_stream() { return g.user_stream ? g.user_stream : g.stream; }
+
+template <class T>
+int dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (!count) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+  return GPULDA_OK;
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+int check_status() {
+  u32 st = 0;
+  CK(cudaMemcpy(&st, g.status, sizeof st, cudaMemcpyDeviceToHost));
+  if (st) {
+    CK(cudaMemset(g.status, 0, sizeof(u32)));
+    char buf[200];
+    snprintf(buf, sizeof buf, "device status 0x%x (%s%s%s%s)", st, (st & kStatusBadTopic) ? "topic>=K " : "",
+             (st & kStatusBadWord) ? "word>=V " : "", (st & kStatusDocRange) ? "document past n_tokens " : "",
+             (st & kStatusDocTooLong) ? "document too long " : "");
+    return fail(GPULDA_ERR_DEVICE, buf);
+  }
+  return GPULDA_OK;
+}
+
+void free_model() {
+  dfree(g.dev.n);
+  dfree(g.dev.q);
+  dfree(g.dev.al);
+  dfree(g.dev.A);
+  dfree(g.dev.S);
+  dfree(g.dev.nnz);
+  dfree(g.C);
+  dfree(g.cdf);
+  dfree(g.guide);
+  dfree(g.lfac);
+  dfree(g.counters);
+  dfree(g.ll);
+  dfree(g.work);
+  dfree(g.status);
+  dfree(g.alias_scratch);
+  dfree(g.cz);
+  dfree(g.cw);
+  dfree(g.cd_len);
+  dfree(g.cd_idx);
+  dfree(g.cK_d);
+  for (auto& e : g.ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : g.z_ev)
+    if (e) cudaEventDestroy(e);
+  if (g.stream) cudaStreamDestroy(g.stream);
+  const int fatal = g.fatal;
+  g = Model();
+  g.fatal = fatal;
+}
+
+int validate_args(const Args* a) {
+  if (!a) return fail(GPULDA_ERR_ARGS, "null Args");
+  if (a->K < 1 || a->V < 1) return fail(GPULDA_ERR_ARGS, "K and V must be positive");
+  if (a->K > GPULDA_MAX_K) return fail(GPULDA_ERR_UNSUPPORTED, "K above GPULDA_MAX_K");
+  if (!(a->alpha > 0.0f) || !(a->beta >= 0.0f) || !std::isfinite(a->alpha) || !std::isfinite(a->beta))
+    return fail(GPULDA_ERR_ARGS, "alpha must be > 0 and beta >= 0");
+  if (a->buffer_size < 1 || a->max_D < 1) return fail(GPULDA_ERR_ARGS, "buffer_size and max_D must be positive");
+  if (!a->C) return fail(GPULDA_ERR_ARGS, "null word counts C");
+  return GPULDA_OK;
+}
+
+int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExArgs* ex) {
+  if (g.live) return fail(GPULDA_ERR_STATE, "initialize called twice without cleanup");
+  int rc = validate_args(args);
+  if (rc) return rc;
+  const int fatal = g.fatal;
+  g = Model();
+  g.fatal = fatal;
+  g.K = args->K;
+  g.V = args->V;
+  g.alpha = args->alpha;
+  g.beta = args->beta;
+  g.buffer_size = args->buffer_size;
+  g.max_D = args->max_D;
+  g.key0 = ex ? (u32)ex->seed : 0u;
+  g.key1 = ex ? ex->chain : 0u;
+  g.flags = ex ? ex->flags : 0u;
+  const size_t cells = (size_t)g.K * g.V;
+
+  CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+  for (auto& e : g.ev) CK(cudaEventCreate(&e));
+  for (auto& e : g.z_ev) CK(cudaEventCreate(&e));
+  if ((rc = dalloc(&g.dev.n, cells)) || (rc = dalloc(&g.dev.q, cells)) || (rc = dalloc(&g.dev.al, cells)) ||
+      (rc = dalloc(&g.dev.A, g.V)) || (rc = dalloc(&g.dev.S, g.K)) || (rc = dalloc(&g.dev.nnz, g.V)) ||
+      (rc = dalloc(&g.C, g.V)) || (rc = dalloc(&g.cdf, (size_t)kPoisN * kPoisW)) ||
+      (rc = dalloc(&g.guide, (size_t)kPoisN * 256)) || (rc = dalloc(&g.lfac, kLogFacN)) ||
+      (rc = dalloc(&g.counters, kCtrN)) || (rc = dalloc(&g.ll, 2)) || (rc = dalloc(&g.work, 1)) ||
+      (rc = dalloc(&g.status, 1))) {
+    free_model();
+    return rc;
+  }
+  g.alias_scratch_bytes = alias_build_scratch_bytes(g.K);
+  if (g.alias_scratch_bytes && (rc = dalloc((unsigned char**)&g.alias_scratch, g.alias_scratch_bytes))) {
+    free_model();
+    return rc;
+  }
+  std::vector<u32> cdf((size_t)kPoisN * kPoisW);
+  std::vector<uint8_t> guide((size_t)kPoisN * 256);
+  std::vector<double> lfac(kLogFacN);
+  build_poisson_tables(g.beta, kPoisN, kPoisW, cdf.data(), guide.data());
+  build_log_factorials(kLogFacN, lfac.data());
+  CK(cudaMemcpy(g.cdf, cdf.data(), cdf.size() * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(g.guide, guide.data(), guide.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(g.lfac, lfac.data(), lfac.size() * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(g.C, args->C, (size_t)g.V * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemset(g.status, 0, 4));
+  CK(cudaMemset(g.counters, 0, kCtrN * 8));
+  CK(cudaMemset(g.ll, 0, 16));
+
+  g.dev.K = g.K;
+  g.dev.V = g.V;
+  g.dev.alpha = g.alpha;
+  g.dev.beta = g.beta;
+  g.dev.key0 = g.key0;
+  g.dev.key1 = g.key1;
+  g.dev.tables = PoisTables{g.cdf, g.guide, g.lfac};
+
+  for (u32 i = 0; i < n_buffers; ++i) {
+    Buffer& b = buffers[i];
+    BufCtx* ctx = new BufCtx();
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
+    cudaStream_t* sp = new cudaStream_t(ctx->stream);
+    b.stream = sp;
+    b.gpu_rng = ctx;
+    u32 *z, *w, *dl, *di, *kd;
+    if ((rc = dalloc(&z, g.buffer_size)) || (rc = dalloc(&w, g.buffer_size)) || (rc = dalloc(&dl, g.max_D)) ||
+        (rc = dalloc(&di, g.max_D)) || (rc = dalloc(&kd, g.max_D)))
+      return rc;
+    b.gpu_z = z;
+    b.gpu_w = w;
+    b.gpu_d_len = dl;
+    b.gpu_d_idx = di;
+    b.gpu_K_d = kd;
+  }
+
+  launch_init_counts(g.dev, g.C, g.stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(g.stream));
+  g.live = true;
+  return GPULDA_OK;
+}
+
+// Phi step on `s` without a host synchronisation.
+int phi_step_async(cudaStream_t s) {
+  g.t += 1;
+  g.tok_offset = 0;
+  g.swept = false;
+  g.launches = 0;
+  CK(cudaEventRecord(g.ev[0], s));
+  CK(cudaMemsetAsync(g.dev.S, 0, (size_t)g.K * 8, s));
+  CK(cudaMemsetAsync(g.counters, 0, kCtrN * 8, s));
+  CK(cudaMemsetAsync(g.ll, 0, 16, s));
+  CK(cudaEventRecord(g.ev[1], s));
+  launch_phi_draw(g.dev, (u32)g.t, s);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(g.ev[2], s));
+  launch_alias_build(g.dev, s, g.alias_scratch, g.alias_scratch_bytes);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(g.ev[3], s));
+  g.launches += 2;
+  g.phi_timed = true;
+  return GPULDA_OK;
+}
+
+// One sweep over documents already on the device.
+int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_idx, u32* K_d, u32 n_docs,
+                 u64 n_tokens, bool offsets, cudaEvent_t* ev) {
+  CK(cudaEventRecord(ev[0], s));
+  if (offsets) {
+    launch_doc_offsets(d_len, d_idx, n_docs, s);
+    CK(cudaGetLastError());
+    g.launches += 1;
+  }
+  CK(cudaEventRecord(ev[1], s));
+  CK(cudaMemsetAsync(g.work, 0, 4, s));
+  ZLaunch zl;
+  zl.w = w;
+  zl.z = z;
+  zl.d_len = d_len;
+  zl.d_idx = d_idx;
+  zl.K_d = K_d;
+  zl.n_docs = n_docs;
+  zl.n_tokens = n_tokens;
+  zl.tok_base = g.tok_offset;
+  zl.t = (u32)g.t;
+  zl.flags = (g.flags & GPULDA_FLAG_LOGLIK) ? 1u : 0u;
+  zl.counters = g.counters;
+  zl.ll = g.ll;
+  zl.work = g.work;
+  zl.status = g.status;
+  launch_z_sweep(g.dev, zl, s);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ev[2], s));
+  g.launches += 1;
+  g.tok_offset += n_tokens;
+  g.swept = true;
+  return GPULDA_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// reference ABI
+// ---------------------------------------------------------------------------
+extern "C" void initialize(Args* args, Buffer* buffers, uint32_t n_buffers) {
+  init_impl(args, buffers, n_buffers, nullptr);
+}
+
+extern "C" void sample_phi(void) {
+  if (!g.live) {
+    fail(GPULDA_ERR_STATE, "sample_phi before initialize");
+    return;
+  }
+  cudaStream_t s = main_stream();
+  if (phi_step_async(s)) return;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    cuda_fail(e, "sample_phi");
+    return;
+  }
+  check_status();
+}
+
+extern "C" void sample_z_async(Buffer* b) {
+  if (!g.live || g.t < 0) {
+    fail(GPULDA_ERR_STATE, "sample_z_async before initialize/sample_phi");
+    return;
+  }
+  if (!b || !b->gpu_rng) {
+    fail(GPULDA_ERR_STATE, "buffer was not passed to initialize");
+    return;
+  }
+  if (b->n_tokens > g.buffer_size || b->n_docs > g.max_D) {
+    fail(GPULDA_ERR_BUFFER, "buffer exceeds buffer_size or max_D");
+    return;
+  }
+  if (!b->n_docs) return;
+  if (!b->z || !b->w || !b->d) {
+    fail(GPULDA_ERR_BUFFER, "null host array in buffer");
+    return;
+  }
+  BufCtx* ctx = (BufCtx*)b->gpu_rng;
+  cudaStream_t s = g.user_stream ? g.user_stream : ctx->stream;
+  const size_t tb = (size_t)b->n_tokens * 4, db = (size_t)b->n_docs * 4;
+#define CKV(expr)                          \
+  do {                                     \
+    cudaError_t e_ = (expr);               \
+    if (e_ != cudaSuccess) {               \
+      cuda_fail(e_, #expr);                \
+      return;                              \
+    }                                      \
+  } while (0)
+  CKV(cudaMemcpyAsync(b->gpu_z, b->z, tb, cudaMemcpyHostToDevice, s));
+  CKV(cudaMemcpyAsync(b->gpu_w, b->w, tb, cudaMemcpyHostToDevice, s));
+  CKV(cudaMemcpyAsync(b->gpu_d_len, b->d, db, cudaMemcpyHostToDevice, s));
+  if (b->K_d) CKV(cudaMemcpyAsync(b->gpu_K_d, b->K_d, db, cudaMemcpyHostToDevice, s));
+  if (z_step_async(s, (u32*)b->gpu_z, (const u32*)b->gpu_w, (const u32*)b->gpu_d_len, (u32*)b->gpu_d_idx,
+                   (u32*)b->gpu_K_d, b->n_docs, b->n_tokens, true, g.z_ev))
+    return;
+  g.z_timed = true;
+  CKV(cudaMemcpyAsync(b->z, b->gpu_z, tb, cudaMemcpyDeviceToHost, s));
+  ctx->used = true;
+#undef CKV
+}
+
+extern "C" void sync_buffer(Buffer* b) {
+  if (!g.live || !b || !b->gpu_rng) {
+    fail(GPULDA_ERR_STATE, "sync_buffer on an unknown buffer");
+    return;
+  }
+  BufCtx* ctx = (BufCtx*)b->gpu_rng;
+  cudaStream_t s = g.user_stream ? g.user_stream : ctx->stream;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    cuda_fail(e, "sync_buffer");
+    return;
+  }
+  check_status();
+}
+
+extern "C" void cleanup(Buffer* buffers, uint32_t n_buffers) {
+  if (!g.live) {
+    fail(GPULDA_ERR_STATE, "cleanup before initialize");
+    return;
+  }
+  cudaDeviceSynchronize();
+  for (u32 i = 0; buffers && i < n_buffers; ++i) {
+    Buffer& b = buffers[i];
+    dfree(b.gpu_z);
+    dfree(b.gpu_w);
+    dfree(b.gpu_d_len);
+    dfree(b.gpu_d_idx);
+    dfree(b.gpu_K_d);
+    if (b.gpu_rng) {
+      BufCtx* ctx = (BufCtx*)b.gpu_rng;
+      for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+      if (ctx->stream) cudaStreamDestroy(ctx->stream);
+      delete ctx;
+    }
+    delete (cudaStream_t*)b.stream;
+    b.gpu_z = b.gpu_w = b.gpu_d_len = b.gpu_d_idx = b.gpu_K_d = b.gpu_rng = b.stream = nullptr;
+  }
+  free_model();
+}
+
+// ---------------------------------------------------------------------------
+// additions
+// ---------------------------------------------------------------------------
+extern "C" int gpulda_last_error(void) {
+  const int e = g.last_error;
+  g.last_error = GPULDA_OK;
+  return e;
+}
+
+extern "C" const char* gpulda_error_string(int code) {
+  if (code < 0 || code > GPULDA_ERR_UNSUPPORTED) return "unknown error";
+  return kErrNames[code];
+}
+
+extern "C" void gpulda_set_fatal_errors(int fatal) { g.fatal = fatal ? 1 : 0; }
+
+extern "C" int gpulda_initialize_ex(const Args* args, Buffer* buffers, uint32_t n_buffers, const GpuldaExArgs* ex) {
+  const int fatal = g.fatal;
+  g.fatal = 0;
+  const int rc = init_impl(args, buffers, n_buffers, ex);
+  g.fatal = fatal;
+  return rc;
+}
+
+extern "C" int gpulda_set_stream(void* s) {
+  g.user_stream = (cudaStream_t)s;
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_loglik(double* out, uint64_t* n_skipped) {
+  if (!g.live || !g.swept) return fail(GPULDA_ERR_STATE, "no completed sweep");
+  if (!(g.flags & GPULDA_FLAG_LOGLIK)) return fail(GPULDA_ERR_STATE, "model initialized without GPULDA_FLAG_LOGLIK");
+  CK(cudaDeviceSynchronize());
+  double h[2];
+  CK(cudaMemcpy(h, g.ll, 16, cudaMemcpyDeviceToHost));
+  if (out) *out = h[0];
+  if (n_skipped) *n_skipped = (uint64_t)h[1];
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_corpus_load(const uint32_t* z, const uint32_t* w, const uint32_t* d_len, uint32_t n_docs,
+                                  uint64_t n_tokens) {
+  if (!g.live) return fail(GPULDA_ERR_STATE, "corpus_load before initialize");
+  if (!z || !w || !d_len) return fail(GPULDA_ERR_ARGS, "null corpus array");
+  if (n_tokens >= (1ull << 32)) return fail(GPULDA_ERR_UNSUPPORTED, "corpus above 2^32 tokens");
+  dfree(g.cz);
+  dfree(g.cw);
+  dfree(g.cd_len);
+  dfree(g.cd_idx);
+  dfree(g.cK_d);
+  g.cz = g.cw = g.cd_len = g.cd_idx = g.cK_d = nullptr;
+  int rc;
+  if ((rc = dalloc(&g.cz, n_tokens)) || (rc = dalloc(&g.cw, n_tokens)) || (rc = dalloc(&g.cd_len, n_docs)) ||
+      (rc = dalloc(&g.cd_idx, n_docs)) || (rc = dalloc(&g.cK_d, n_docs)))
+    return rc;
+  CK(cudaMemcpy(g.cz, z, n_tokens * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(g.cw, w, n_tokens * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(g.cd_len, d_len, (size_t)n_docs * 4, cudaMemcpyHostToDevice));
+  launch_doc_offsets(g.cd_len, g.cd_idx, n_docs, g.stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(g.stream));
+  g.c_docs = n_docs;
+  g.c_tokens = n_tokens;
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_corpus_sweep(uint32_t n_iter) {
+  if (!g.live || !g.cz) return fail(GPULDA_ERR_STATE, "corpus_sweep without a loaded corpus");
+  cudaStream_t s = main_stream();
+  for (u32 i = 0; i < n_iter; ++i) {
+    int rc = phi_step_async(s);
+    if (rc) return rc;
+    rc = z_step_async(s, g.cz, g.cw, g.cd_len, g.cd_idx, g.cK_d, g.c_docs, g.c_tokens, false, g.z_ev);
+    if (rc) return rc;
+    g.z_timed = true;
+  }
+  CK(cudaStreamSynchronize(s));
+  return check_status();
+}
+
+extern "C" int gpulda_corpus_read_z(uint32_t* z_out) {
+  if (!g.live || !g.cz) return fail(GPULDA_ERR_STATE, "no corpus loaded");
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(z_out, g.cz, g.c_tokens * 4, cudaMemcpyDeviceToHost));
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_kernel_times(float* ms, int n) {
+  if (!g.live) return 0;
+  float v[kTN] = {0, 0, 0, 0, 0};
+  if (g.phi_timed) {
+    cudaEventSynchronize(g.ev[3]);
+    cudaEventElapsedTime(&v[kTPrep], g.ev[0], g.ev[1]);
+    cudaEventElapsedTime(&v[kTPhi], g.ev[1], g.ev[2]);
+    cudaEventElapsedTime(&v[kTAlias], g.ev[2], g.ev[3]);
+  }
+  if (g.z_timed) {
+    cudaEventSynchronize(g.z_ev[2]);
+    cudaEventElapsedTime(&v[kTOffsets], g.z_ev[0], g.z_ev[1]);
+    cudaEventElapsedTime(&v[kTZ], g.z_ev[1], g.z_ev[2]);
+  }
+  int m = n < kTN ? n : kTN;
+  for (int i = 0; i < m; ++i) ms[i] = v[i];
+  return m;
+}
+
+extern "C" int gpulda_counters(uint64_t* out, int n) {
+  if (!g.live) return 0;
+  unsigned long long h[kCtrN];
+  if (cudaDeviceSynchronize() != cudaSuccess) return 0;
+  if (cudaMemcpy(h, g.counters, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+  uint64_t v[kCtrN + 1];
+  for (int i = 0; i < kCtrN; ++i) v[i] = h[i];
+  v[kCtrN] = g.launches;
+  int m = n < kCtrN + 1 ? n : kCtrN + 1;
+  for (int i = 0; i < m; ++i) out[i] = v[i];
+  return m;
+}
+
+extern "C" int gpulda_debug_read(uint32_t* n, uint32_t* q, uint64_t* alias, uint64_t* A, uint64_t* S, uint32_t* nnz) {
+  if (!g.live) return fail(GPULDA_ERR_STATE, "debug_read before initialize");
+  CK(cudaDeviceSynchronize());
+  const size_t cells = (size_t)g.K * g.V;
+  if (n) CK(cudaMemcpy(n, g.dev.n, cells * 4, cudaMemcpyDeviceToHost));
+  if (q) CK(cudaMemcpy(q, g.dev.q, cells * 4, cudaMemcpyDeviceToHost));
+  if (alias) CK(cudaMemcpy(alias, g.dev.al, cells * 8, cudaMemcpyDeviceToHost));
+  if (A) CK(cudaMemcpy(A, g.dev.A, (size_t)g.V * 8, cudaMemcpyDeviceToHost));
+  if (S) CK(cudaMemcpy(S, g.dev.S, (size_t)g.K * 8, cudaMemcpyDeviceToHost));
+  if (nnz) CK(cudaMemcpy(nnz, g.dev.nnz, (size_t)g.V * 4, cudaMemcpyDeviceToHost));
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_debug_write_counts(const uint32_t* n) {
+  if (!g.live) return fail(GPULDA_ERR_STATE, "debug_write_counts before initialize");
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(g.dev.n, n, (size_t)g.K * g.V * 4, cudaMemcpyHostToDevice));
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_debug_tables(uint32_t* cdf, double* lfac) {
+  if (!g.live) return fail(GPULDA_ERR_STATE, "debug_tables before initialize");
+  if (cdf) CK(cudaMemcpy(cdf, g.cdf, (size_t)kPoisN * kPoisW * 4, cudaMemcpyDeviceToHost));
+  if (lfac) CK(cudaMemcpy(lfac, g.lfac, (size_t)kLogFacN * 8, cudaMemcpyDeviceToHost));
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_debug_philox(const uint32_t* ctr, uint32_t n, uint32_t key0, uint32_t key1, uint32_t* out) {
+  if (!n) return GPULDA_OK;
+  u32 *dc = nullptr, *dout = nullptr;
+  int rc;
+  if ((rc = dalloc(&dc, (size_t)n * 4)) || (rc = dalloc(&dout, (size_t)n * 4))) {
+    dfree(dc);
+    return rc;
+  }
+  cudaMemcpy(dc, ctr, (size_t)n * 16, cudaMemcpyHostToDevice);
+  launch_debug_philox(dc, n, key0, key1, dout, 0);
+  cudaError_t e = cudaMemcpy(out, dout, (size_t)n * 16, cudaMemcpyDeviceToHost);
+  dfree(dc);
+  dfree(dout);
+  if (e != cudaSuccess) return cuda_fail(e, "debug_philox");
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_debug_poisson(const uint32_t* count, const uint64_t* idx, uint32_t n, uint32_t t,
+                                    uint32_t stream, uint32_t key0, uint32_t key1, uint32_t* out) {
+  if (!g.live) return fail(GPULDA_ERR_STATE, "debug_poisson before initialize");
+  if (!n) return GPULDA_OK;
+  u32 *dc = nullptr, *dout = nullptr;
+  u64* di = nullptr;
+  int rc;
+  if ((rc = dalloc(&dc, n)) || (rc = dalloc(&dout, n)) || (rc = dalloc(&di, n))) {
+    dfree(dc);
+    dfree(dout);
+    return rc;
+  }
+  cudaMemcpy(dc, count, (size_t)n * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(di, idx, (size_t)n * 8, cudaMemcpyHostToDevice);
+  launch_debug_poisson(g.dev, dc, di, n, t, stream, key0, key1, dout, 0);
+  cudaError_t e = cudaMemcpy(out, dout, (size_t)n * 4, cudaMemcpyDeviceToHost);
+  dfree(dc);
+  dfree(dout);
+  dfree(di);
+  if (e != cudaSuccess) return cuda_fail(e, "debug_poisson");
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_debug_alias(const uint32_t* q, uint32_t K, uint64_t* table_out) {
+  if (K < 1 || K > 12288) return fail(GPULDA_ERR_UNSUPPORTED, "debug_alias supports 1 <= K <= 12288");
+  u32* dq = nullptr;
+  u64* dout = nullptr;
+  int rc;
+  if ((rc = dalloc(&dq, K)) || (rc = dalloc(&dout, K))) {
+    dfree(dq);
+    return rc;
+  }
+  cudaMemcpy(dq, q, (size_t)K * 4, cudaMemcpyHostToDevice);
+  launch_debug_alias(dq, K, dout, 0);
+  cudaError_t e = cudaMemcpy(table_out, dout, (size_t)K * 8, cudaMemcpyDeviceToHost);
+  dfree(dq);
+  dfree(dout);
+  if (e != cudaSuccess) return cuda_fail(e, "debug_alias");
+  return GPULDA_OK;
+}
