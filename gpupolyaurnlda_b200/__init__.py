@@ -105,6 +105,8 @@ _SIGNATURES = {
     "gpulda_debug_poisson": (C.c_int, [_U32P, _U64P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                        C.c_uint32, _U32P]),
     "gpulda_debug_alias": (C.c_int, [_U32P, C.c_uint32, _U64P]),
+    "gpulda_sample_z_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
+                                                 C.c_void_p]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGNATURES)

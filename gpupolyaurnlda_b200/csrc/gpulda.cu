@@ -626,3 +626,75 @@ extern "C" int gpulda_debug_alias(const uint32_t* q, uint32_t K, uint64_t* table
   if (e != cudaSuccess) return cuda_fail(e, "debug_alias");
   return GPULDA_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free sweep over documents that are already in device memory.
+//
+// For callers that may not allocate device memory at the point of the call:
+// code that owns all device memory through its own pool, services that must
+// not allocate once serving has started, or work issued where cudaMalloc is
+// not permitted.  Its only scratch (document offsets and the work-queue
+// counter) is the file-scope device array below, sized for
+// GPULDA_NOALLOC_MAX_DOCS documents: 4 MiB + 256 B that every GPU which loads
+// this library holds until the process exits.  In host code the array's name
+// is only a host-side stand-in; its device address is looked up once per
+// device with cudaGetSymbolAddress (on the first call on that device, which
+// is why that first call should come before any stream capture).  All calls
+// share the array, so calls whose work overlaps on the GPU race with each
+// other; the work-queue counter is cleared on every call.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr u32 kNoAllocMaxDocs = GPULDA_NOALLOC_MAX_DOCS;
+constexpr u32 kNoAllocTail = 64;  // work-queue counter and padding
+static __device__ __align__(256) u32 g_noalloc_scratch[kNoAllocMaxDocs + kNoAllocTail];
+constexpr int kNoAllocMaxDevices = 64;
+u32* g_noalloc_addr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+extern "C" int gpulda_sample_z_device_noalloc(uint32_t* z, const uint32_t* w, const uint32_t* d_len,
+                                              uint32_t n_docs, uint64_t n_tokens, void* stream) {
+  if (!g.live || g.t < 0) return fail(GPULDA_ERR_STATE, "gpulda_sample_z_device_noalloc before initialize/sample_phi");
+  if (n_docs > kNoAllocMaxDocs)
+    return fail(GPULDA_ERR_UNSUPPORTED,
+                "gpulda_sample_z_device_noalloc: n_docs exceeds GPULDA_NOALLOC_MAX_DOCS (1048576 documents)");
+  if (n_tokens >= (1ull << 32))
+    return fail(GPULDA_ERR_UNSUPPORTED, "gpulda_sample_z_device_noalloc: n_tokens must be below 2^32");
+  if (!n_docs) return GPULDA_OK;
+  if (!z || !w || !d_len) return fail(GPULDA_ERR_ARGS, "gpulda_sample_z_device_noalloc: null device array");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(GPULDA_ERR_UNSUPPORTED, "gpulda_sample_z_device_noalloc: device ordinal above 63");
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_addr[dev] = (u32*)p;
+  }
+  u32* d_idx = g_noalloc_addr[dev];
+  u32* work = d_idx + kNoAllocMaxDocs;
+  cudaStream_t s = stream ? (cudaStream_t)stream : main_stream();
+  CK(cudaMemsetAsync(work, 0, sizeof(u32), s));
+  launch_doc_offsets(d_len, d_idx, n_docs, s);
+  CK(cudaGetLastError());
+  ZLaunch zl;
+  zl.w = w;
+  zl.z = z;
+  zl.d_len = d_len;
+  zl.d_idx = d_idx;
+  zl.K_d = nullptr;
+  zl.n_docs = n_docs;
+  zl.n_tokens = n_tokens;
+  zl.tok_base = g.tok_offset;
+  zl.t = (u32)g.t;
+  zl.flags = (g.flags & GPULDA_FLAG_LOGLIK) ? 1u : 0u;
+  zl.counters = g.counters;
+  zl.ll = g.ll;
+  zl.work = work;
+  zl.status = g.status;
+  launch_z_sweep(g.dev, zl, s);
+  CK(cudaGetLastError());
+  g.tok_offset += n_tokens;
+  g.swept = true;
+  return GPULDA_OK;
+}

@@ -204,6 +204,30 @@ int gpulda_debug_poisson(const uint32_t* count, const uint64_t* idx, uint32_t n,
  * the library's parallel construction; writes K packed entries. */
 int gpulda_debug_alias(const uint32_t* q, uint32_t K, uint64_t* table_out);
 
+/* ---- allocation-free sweep ------------------------------------------------
+ * No counterpart in the reference: an addition for callers that must not
+ * allocate device memory when they call (a host application that owns all
+ * device memory through its own pool, a service that allocates nothing once
+ * it is serving, or work issued where cudaMalloc is not permitted).
+ *
+ * Sweeps n_docs documents whose topics z (read and rewritten), words w and
+ * lengths d_len are already in device memory, exactly as sample_z_async
+ * sweeps a buffer (same draws, same count rebuild, continuing the current
+ * iteration's token numbering).  Asynchronous on `stream` (NULL: the
+ * library's stream); device-side input errors are reported by the next
+ * sync_buffer / sample_phi / gpulda_corpus_* call.
+ *
+ * It allocates nothing: its scratch (document offsets and a work counter) is
+ * a fixed device array of the library, 4 MiB + 256 B held by every GPU that
+ * loads the library until the process exits.  n_docs above
+ * GPULDA_NOALLOC_MAX_DOCS is rejected with GPULDA_ERR_UNSUPPORTED.  The first
+ * call on a device looks up that array's address, so make the first call
+ * before any stream capture.  Calls share the array: calls whose work
+ * overlaps on the GPU race with each other. */
+#define GPULDA_NOALLOC_MAX_DOCS 1048576u
+int gpulda_sample_z_device_noalloc(uint32_t* z, const uint32_t* w, const uint32_t* d_len, uint32_t n_docs,
+                                   uint64_t n_tokens, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
