@@ -35,7 +35,23 @@ struct BufCtx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   bool used = false;
+  u32* order = nullptr;           // device: document processing order
+  std::vector<u32> order_host;    // host staging of the order
 };
+
+// Documents longest first (counting sort on length, ties in index order), so
+// the longest sequential chains start first and the sweep's tail is short.
+// The order does not change any result: documents are independent and the
+// count rebuild is an integer sum.
+void longest_first(const u32* d_len, u32 n, std::vector<u32>& order) {
+  order.resize(n);
+  u32 max_len = 0;
+  for (u32 i = 0; i < n; ++i) max_len = std::max(max_len, d_len[i]);
+  std::vector<u32> start((size_t)max_len + 2, 0);
+  for (u32 i = 0; i < n; ++i) start[max_len - d_len[i] + 1]++;
+  for (size_t b = 1; b < start.size(); ++b) start[b] += start[b - 1];
+  for (u32 i = 0; i < n; ++i) order[start[max_len - d_len[i]]++] = i;
+}
 
 struct Model {
   bool live = false;
@@ -69,7 +85,7 @@ struct Model {
   u32 launches = 0;
 
   // device-resident corpus
-  u32 *cz = nullptr, *cw = nullptr, *cd_len = nullptr, *cd_idx = nullptr, *cK_d = nullptr;
+  u32 *cz = nullptr, *cw = nullptr, *cd_len = nullptr, *cd_idx = nullptr, *cK_d = nullptr, *corder = nullptr;
   u32 c_docs = 0;
   u64 c_tokens = 0;
 };
@@ -139,6 +155,7 @@ void free_model() {
   dfree(g.dev.n);
   dfree(g.dev.q);
   dfree(g.dev.al);
+  dfree(g.dev.csr);
   dfree(g.dev.A);
   dfree(g.dev.S);
   dfree(g.dev.nnz);
@@ -156,6 +173,7 @@ void free_model() {
   dfree(g.cd_len);
   dfree(g.cd_idx);
   dfree(g.cK_d);
+  dfree(g.corder);
   for (auto& e : g.ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : g.z_ev)
@@ -199,6 +217,7 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
   for (auto& e : g.ev) CK(cudaEventCreate(&e));
   for (auto& e : g.z_ev) CK(cudaEventCreate(&e));
   if ((rc = dalloc(&g.dev.n, cells)) || (rc = dalloc(&g.dev.q, cells)) || (rc = dalloc(&g.dev.al, cells)) ||
+      (rc = dalloc(&g.dev.csr, cells)) ||
       (rc = dalloc(&g.dev.A, g.V)) || (rc = dalloc(&g.dev.S, g.K)) || (rc = dalloc(&g.dev.nnz, g.V)) ||
       (rc = dalloc(&g.C, g.V)) || (rc = dalloc(&g.cdf, (size_t)kPoisN * kPoisW)) ||
       (rc = dalloc(&g.guide, (size_t)kPoisN * 256)) || (rc = dalloc(&g.lfac, kLogFacN)) ||
@@ -243,7 +262,7 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
     b.gpu_rng = ctx;
     u32 *z, *w, *dl, *di, *kd;
     if ((rc = dalloc(&z, g.buffer_size)) || (rc = dalloc(&w, g.buffer_size)) || (rc = dalloc(&dl, g.max_D)) ||
-        (rc = dalloc(&di, g.max_D)) || (rc = dalloc(&kd, g.max_D)))
+        (rc = dalloc(&di, g.max_D)) || (rc = dalloc(&kd, g.max_D)) || (rc = dalloc(&ctx->order, g.max_D)))
       return rc;
     b.gpu_z = z;
     b.gpu_w = w;
@@ -282,8 +301,8 @@ int phi_step_async(cudaStream_t s) {
 }
 
 // One sweep over documents already on the device.
-int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_idx, u32* K_d, u32 n_docs,
-                 u64 n_tokens, bool offsets, cudaEvent_t* ev) {
+int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_idx, const u32* order, u32* K_d,
+                 u32 n_docs, u64 n_tokens, bool offsets, cudaEvent_t* ev) {
   CK(cudaEventRecord(ev[0], s));
   if (offsets) {
     launch_doc_offsets(d_len, d_idx, n_docs, s);
@@ -297,6 +316,7 @@ int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_
   zl.z = z;
   zl.d_len = d_len;
   zl.d_idx = d_idx;
+  zl.order = order;
   zl.K_d = K_d;
   zl.n_docs = n_docs;
   zl.n_tokens = n_tokens;
@@ -373,8 +393,13 @@ extern "C" void sample_z_async(Buffer* b) {
   CKV(cudaMemcpyAsync(b->gpu_w, b->w, tb, cudaMemcpyHostToDevice, s));
   CKV(cudaMemcpyAsync(b->gpu_d_len, b->d, db, cudaMemcpyHostToDevice, s));
   if (b->K_d) CKV(cudaMemcpyAsync(b->gpu_K_d, b->K_d, db, cudaMemcpyHostToDevice, s));
+  // This buffer's previous copy out of order_host must finish before it is rewritten.
+  if (ctx->used) CKV(cudaEventSynchronize(ctx->ev[0]));
+  longest_first(b->d, b->n_docs, ctx->order_host);
+  CKV(cudaMemcpyAsync(ctx->order, ctx->order_host.data(), db, cudaMemcpyHostToDevice, s));
+  CKV(cudaEventRecord(ctx->ev[0], s));
   if (z_step_async(s, (u32*)b->gpu_z, (const u32*)b->gpu_w, (const u32*)b->gpu_d_len, (u32*)b->gpu_d_idx,
-                   (u32*)b->gpu_K_d, b->n_docs, b->n_tokens, true, g.z_ev))
+                   ctx->order, (u32*)b->gpu_K_d, b->n_docs, b->n_tokens, true, g.z_ev))
     return;
   g.z_timed = true;
   CKV(cudaMemcpyAsync(b->z, b->gpu_z, tb, cudaMemcpyDeviceToHost, s));
@@ -415,6 +440,7 @@ extern "C" void cleanup(Buffer* buffers, uint32_t n_buffers) {
       for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
       if (ctx->stream) cudaStreamDestroy(ctx->stream);
+      dfree(ctx->order);
       delete ctx;
     }
     delete (cudaStream_t*)b.stream;
@@ -473,14 +499,18 @@ extern "C" int gpulda_corpus_load(const uint32_t* z, const uint32_t* w, const ui
   dfree(g.cd_len);
   dfree(g.cd_idx);
   dfree(g.cK_d);
-  g.cz = g.cw = g.cd_len = g.cd_idx = g.cK_d = nullptr;
+  dfree(g.corder);
+  g.cz = g.cw = g.cd_len = g.cd_idx = g.cK_d = g.corder = nullptr;
   int rc;
   if ((rc = dalloc(&g.cz, n_tokens)) || (rc = dalloc(&g.cw, n_tokens)) || (rc = dalloc(&g.cd_len, n_docs)) ||
-      (rc = dalloc(&g.cd_idx, n_docs)) || (rc = dalloc(&g.cK_d, n_docs)))
+      (rc = dalloc(&g.cd_idx, n_docs)) || (rc = dalloc(&g.cK_d, n_docs)) || (rc = dalloc(&g.corder, n_docs)))
     return rc;
   CK(cudaMemcpy(g.cz, z, n_tokens * 4, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(g.cw, w, n_tokens * 4, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(g.cd_len, d_len, (size_t)n_docs * 4, cudaMemcpyHostToDevice));
+  std::vector<u32> order;
+  longest_first(d_len, n_docs, order);
+  CK(cudaMemcpy(g.corder, order.data(), (size_t)n_docs * 4, cudaMemcpyHostToDevice));
   launch_doc_offsets(g.cd_len, g.cd_idx, n_docs, g.stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(g.stream));
@@ -495,7 +525,7 @@ extern "C" int gpulda_corpus_sweep(uint32_t n_iter) {
   for (u32 i = 0; i < n_iter; ++i) {
     int rc = phi_step_async(s);
     if (rc) return rc;
-    rc = z_step_async(s, g.cz, g.cw, g.cd_len, g.cd_idx, g.cK_d, g.c_docs, g.c_tokens, false, g.z_ev);
+    rc = z_step_async(s, g.cz, g.cw, g.cd_len, g.cd_idx, g.corder, g.cK_d, g.c_docs, g.c_tokens, false, g.z_ev);
     if (rc) return rc;
     g.z_timed = true;
   }
@@ -682,6 +712,7 @@ extern "C" int gpulda_sample_z_device_noalloc(uint32_t* z, const uint32_t* w, co
   zl.z = z;
   zl.d_len = d_len;
   zl.d_idx = d_idx;
+  zl.order = nullptr;
   zl.K_d = nullptr;
   zl.n_docs = n_docs;
   zl.n_tokens = n_tokens;

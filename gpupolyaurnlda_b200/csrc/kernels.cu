@@ -9,6 +9,7 @@
 //                 p(k) ~ q[w_i][k] * (alpha + m_dk), add back, n[w_i][z_i] += 1
 // All arrays indexed by (word, topic) are word-major: index w*K + k.
 #include "kernels.cuh"
+#include "warp.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -17,58 +18,6 @@
 namespace gpulda {
 
 namespace {
-
-constexpr u32 kMaxDocLen = 65535u;
-
-__device__ __forceinline__ u64 warp_incl_scan_u64(u64 x, u32 lane) {
-#pragma unroll
-  for (u32 o = 1; o < 32; o <<= 1) {
-    const u64 y = __shfl_up_sync(kFullMask, x, o);
-    if (lane >= o) x += y;
-  }
-  return x;
-}
-
-__device__ __forceinline__ u64 warp_sum_u64(u64 x) {
-#pragma unroll
-  for (u32 o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFullMask, x, o);
-  return x;
-}
-
-__device__ __forceinline__ double warp_sum_f64(double x) {
-#pragma unroll
-  for (u32 o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFullMask, x, o);
-  return x;
-}
-
-// Block-wide exclusive scan of one u64 per thread; `sh` holds 33 entries.
-__device__ __forceinline__ u64 block_excl_scan_u64(u64 v, u64* sh, u64* total) {
-  const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const u64 incl = warp_incl_scan_u64(v, lane);
-  if (lane == 31) sh[warp] = incl;
-  __syncthreads();
-  if (warp == 0) {
-    u64 x = lane < nw ? sh[lane] : 0;
-    x = warp_incl_scan_u64(x, lane);
-    sh[lane] = x;
-  }
-  __syncthreads();
-  const u64 off = warp ? sh[warp - 1] : 0;
-  *total = sh[nw - 1];
-  __syncthreads();
-  return off + incl - v;
-}
-
-__device__ __forceinline__ u64 block_sum_u64(u64 v, u64* sh) {
-  const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  v = warp_sum_u64(v);
-  if (lane == 0) sh[warp] = v;
-  __syncthreads();
-  u64 t = 0;
-  for (u32 i = 0; i < nw; ++i) t += sh[i];
-  __syncthreads();
-  return t;
-}
 
 // ---------------------------------------------------------------------------
 // Initial counts (reference: polya_urn_init, src/cu/polyaurn.cu:61-79):
@@ -235,6 +184,17 @@ __global__ void __launch_bounds__(256) alias_build_kernel(ModelDev m, unsigned c
     const u64 A = block_sum_u64(part, sh);
     const u64 nz = block_sum_u64(cnt, sh);
     alias_build_block(sq, K, A, vals, idx, m.al + row, sh);
+    {
+      // the word's nonzero q in ascending k (thread chunks are contiguous)
+      const u32 chunk = (K + blockDim.x - 1) / blockDim.x;
+      const u32 k0 = min(K, threadIdx.x * chunk), k1 = min(K, k0 + chunk);
+      u64 c = 0;
+      for (u32 k = k0; k < k1; ++k) c += sq[k] != 0;
+      u64 tot;
+      u64 pos = block_excl_scan_u64(c, sh, &tot);
+      for (u32 k = k0; k < k1; ++k)
+        if (sq[k]) m.csr[row + pos++] = (sq[k] << 32) | k;
+    }
     if (threadIdx.x == 0) {
       m.A[w] = A;
       m.nnz[w] = (u32)nz;
@@ -275,219 +235,6 @@ __global__ void __launch_bounds__(1024) doc_offsets_kernel(const u32* __restrict
     d_idx[i] = (u32)off;
     off += d_len[i];
   }
-}
-
-// ---------------------------------------------------------------------------
-// z sweep (reference: sample_topics, src/cu/topics.cu:36-105, with
-// count_topics / compute_product_cumsum / draw_wary_search / draw_alias from
-// src/cu/topics.cuh:63-192).  One warp per document; documents come from a
-// global work counter.  The document's topic counts m_d live in shared memory
-// as 16-bit counts plus a bitmap of nonzero topics; lane l owns bitmap words
-// [l*wpl, (l+1)*wpl), i.e. a contiguous topic range, so lane order followed by
-// bit order is ascending topic order.
-//
-// Per token (after removing its current topic):
-//   B      = sum_k m_dk * q[w][k]      (u64, exact)
-//   sparse iff u0 * (alpha*A[w] + B) < B
-//   sparse: target = floor(u1 * B); topic = first k (ascending) whose
-//           inclusive prefix of m_dk * q[w][k] exceeds target
-//   dense:  slot = floor(u2 * K); topic = slot if u3 < threshold else alias
-//   (alpha*A + B == 0: the topic is kept)
-// then the topic is added back and n[w][topic] incremented.
-// ---------------------------------------------------------------------------
-struct ZKernelArgs {
-  ModelDev m;
-  ZLaunch z;
-  u32 wpl;
-  double lg_Ka;  // lgamma(K * alpha)
-  double lg_a;   // lgamma(alpha)
-};
-
-__global__ void __launch_bounds__(256) z_sweep_kernel(ZKernelArgs a) {
-  extern __shared__ __align__(16) unsigned char zsm[];
-  const ModelDev& m = a.m;
-  const ZLaunch& p = a.z;
-  const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const u32 K = m.K, V = m.V, wpl = a.wpl;
-  const u32 Kp = (K + 63) & ~63u;
-  const u32 nbw = 32 * wpl;
-  const size_t per_warp = (size_t)Kp * 2 + (size_t)nbw * 4;
-  uint16_t* cnt = (uint16_t*)(zsm + warp * per_warp);
-  u32* bits = (u32*)(zsm + warp * per_warp + (size_t)Kp * 2);
-  const bool want_ll = (p.flags & 1u) && p.ll;
-
-  u64 st_tok = 0, st_docs = 0, st_S = 0, st_sp = 0;
-  double ll_acc = 0.0, ll_skip = 0.0;
-  u32 status = 0;
-
-  while (true) {
-    u32 doc = 0;
-    if (lane == 0) doc = atomicAdd(p.work, 1u);
-    doc = __shfl_sync(kFullMask, doc, 0);
-    if (doc >= p.n_docs) break;
-    const u32 L = p.d_len[doc];
-    const u64 off = p.d_idx[doc];
-    if (L > kMaxDocLen) {
-      status |= kStatusDocTooLong;
-      continue;
-    }
-    if (off + L > p.n_tokens) {
-      status |= kStatusDocRange;
-      continue;
-    }
-    for (u32 i = lane; i < Kp / 8; i += 32) reinterpret_cast<uint4*>(cnt)[i] = make_uint4(0, 0, 0, 0);
-    for (u32 i = lane; i < nbw; i += 32) bits[i] = 0;
-    __syncwarp();
-    for (u32 i = lane; i < L; i += 32) {
-      u32 k = p.z[off + i];
-      if (k >= K) {
-        status |= kStatusBadTopic;
-        k %= K;
-      }
-      atomicAdd(reinterpret_cast<u32*>(cnt) + (k >> 1), 1u << ((k & 1) * 16));
-      atomicOr(bits + (k >> 5), 1u << (k & 31));
-    }
-    __syncwarp();
-    u32 nz = 0;  // distinct topics in the document
-    for (u32 b = 0; b < wpl; ++b) nz += __popc(bits[lane * wpl + b]);
-    nz = (u32)warp_sum_u64(nz);
-
-    for (u32 base = 0; base < L; base += 32) {
-      const u32 i = base + lane;
-      const bool valid = i < L;
-      u32 my_w = valid ? p.w[off + i] : 0;
-      u32 my_z = valid ? p.z[off + i] : 0;
-      if (my_w >= V) {
-        status |= kStatusBadWord;
-        my_w %= V;
-      }
-      if (my_z >= K) my_z %= K;
-      const U4 r = draw4(p.tok_base + off + i, p.t, kStreamZ, 0, m.key0, m.key1);
-      u32 new_z = my_z;
-      const u32 nt = min(32u, L - base);
-      for (u32 j = 0; j < nt; ++j) {
-        const u32 wj = __shfl_sync(kFullMask, my_w, j);
-        const u32 zj = __shfl_sync(kFullMask, my_z, j);
-        const u32 r0 = __shfl_sync(kFullMask, r.x, j);
-        const u32 r1 = __shfl_sync(kFullMask, r.y, j);
-        const u32 r2 = __shfl_sync(kFullMask, r.z, j);
-        const u32 r3 = __shfl_sync(kFullMask, r.w, j);
-        const size_t row = (size_t)wj * K;
-        const u32* __restrict__ qrow = m.q + row;
-        if (lane == 0) {
-          const u32 c = cnt[zj] - 1u;
-          cnt[zj] = (uint16_t)c;
-          if (c == 0) bits[zj >> 5] &= ~(1u << (zj & 31));
-        }
-        __syncwarp();
-        // Sparse mass over this lane's topic range, ascending.
-        u64 ls = 0;
-        u32 myn = 0;
-        for (u32 b = 0; b < wpl; ++b) {
-          const u32 wi = lane * wpl + b;
-          u32 bm = bits[wi];
-          myn += __popc(bm);
-          while (bm) {
-            const u32 k = wi * 32 + (__ffs(bm) - 1);
-            bm &= bm - 1;
-            ls += (u64)cnt[k] * __ldg(qrow + k);
-          }
-        }
-        const u64 incl = warp_incl_scan_u64(ls, lane);
-        const u64 B = __shfl_sync(kFullMask, incl, 31);
-        const u64 Aw = __ldg(m.A + wj);
-        int degenerate;
-        const int sp = take_sparse(r0, m.alpha, Aw, B, &degenerate);
-        u32 k;
-        if (degenerate) {
-          k = zj;
-        } else if (sp) {
-          const u64 target = scale_u32(r1, B);
-          const u32 ball = __ballot_sync(kFullMask, incl > target);
-          const u32 f = __ffs(ball) - 1;
-          u32 kk = 0;
-          if (lane == f) {
-            u64 run = incl - ls;
-            bool done = false;
-            for (u32 b = 0; b < wpl && !done; ++b) {
-              const u32 wi = lane * wpl + b;
-              u32 bm = bits[wi];
-              while (bm) {
-                const u32 kc = wi * 32 + (__ffs(bm) - 1);
-                bm &= bm - 1;
-                run += (u64)cnt[kc] * __ldg(qrow + kc);
-                if (run > target) {
-                  kk = kc;
-                  done = true;
-                  break;
-                }
-              }
-            }
-          }
-          k = __shfl_sync(kFullMask, kk, f);
-        } else {
-          const u32 s = (u32)(((u64)r2 * K) >> 32);
-          const u64 e = __ldg(m.al + row + s);
-          k = alias_pick(e, s, r3);
-        }
-        const u32 ndoc = (u32)warp_sum_u64(myn);  // nnz(m_d) without this token
-        if (lane == 0) {
-          const u32 c = cnt[k] + 1u;
-          cnt[k] = (uint16_t)c;
-          if (c == 1) bits[k >> 5] |= 1u << (k & 31);
-          atomicAdd(m.n + row + k, 1u);
-          const u32 nw = __ldg(m.nnz + wj);
-          st_S += min(ndoc, nw);
-          st_sp += (sp && !degenerate) ? 1 : 0;
-          if (want_ll) {
-            const u32 qk = __ldg(qrow + k);
-            if (qk)
-              ll_acc += log((double)qk) - 22.18070977791825;  // 32 log 2
-            else
-              ll_skip += 1.0;
-          }
-        }
-        if (lane == j) new_z = k;
-        __syncwarp();
-      }
-      if (valid) p.z[off + i] = new_z;
-    }
-    // distinct topics after the sweep
-    u32 nz_end = 0;
-    for (u32 b = 0; b < wpl; ++b) nz_end += __popc(bits[lane * wpl + b]);
-    nz_end = (u32)warp_sum_u64(nz_end);
-    (void)nz;
-    if (lane == 0 && p.K_d) p.K_d[doc] = nz_end;
-    if (want_ll) {
-      double dl = 0.0;
-      for (u32 b = 0; b < wpl; ++b) {
-        const u32 wi = lane * wpl + b;
-        u32 bm = bits[wi];
-        while (bm) {
-          const u32 k = wi * 32 + (__ffs(bm) - 1);
-          bm &= bm - 1;
-          dl += lgamma((double)m.alpha + (double)cnt[k]) - a.lg_a;
-        }
-      }
-      dl = warp_sum_f64(dl);
-      if (lane == 0) ll_acc += dl + a.lg_Ka - lgamma((double)K * (double)m.alpha + (double)L);
-    }
-    st_tok += L;
-    st_docs += 1;
-    __syncwarp();
-  }
-  if (lane == 0) {
-    atomicAdd(p.counters + kCtrTokens, (unsigned long long)st_tok);
-    atomicAdd(p.counters + kCtrDocs, (unsigned long long)st_docs);
-    atomicAdd(p.counters + kCtrSparseWork, (unsigned long long)st_S);
-    atomicAdd(p.counters + kCtrSparseDraws, (unsigned long long)st_sp);
-    if (want_ll) {
-      atomicAdd(p.ll, ll_acc);
-      atomicAdd(p.ll + 1, ll_skip);
-    }
-  }
-  status = __reduce_or_sync(kFullMask, status);
-  if (lane == 0 && status) atomicOr(p.status, status);
 }
 
 __global__ void debug_philox_kernel(const u32* ctr, u32 n, u32 k0, u32 k1, u32* out) {
@@ -571,37 +318,6 @@ void launch_alias_build(const ModelDev& m, cudaStream_t s, void* scratch, size_t
 void launch_doc_offsets(const u32* d_len, u32* d_idx, u32 n_docs, cudaStream_t s) {
   if (!n_docs) return;
   doc_offsets_kernel<<<1, 1024, 0, s>>>(d_len, d_idx, n_docs);
-}
-
-size_t z_sweep_smem_per_warp(u32 K) {
-  const u32 Kp = (K + 63) & ~63u;
-  const u32 nw = (K + 31) / 32;
-  const u32 wpl = (nw + 31) / 32;
-  return (size_t)Kp * 2 + (size_t)32 * wpl * 4;
-}
-
-void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s) {
-  if (!z.n_docs) return;
-  ZKernelArgs a;
-  a.m = m;
-  a.z = z;
-  const u32 nw = (m.K + 31) / 32;
-  a.wpl = (nw + 31) / 32;
-  a.lg_a = lgamma((double)m.alpha);
-  a.lg_Ka = lgamma((double)m.K * (double)m.alpha);
-  const size_t per_warp = z_sweep_smem_per_warp(m.K);
-  // Warps per block: as many as fit 200 KB, at most 8.
-  u32 wpb = 8;
-  while (wpb > 1 && per_warp * wpb > kMaxDynSmem) --wpb;
-  const size_t smem = per_warp * wpb;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(z_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, z_sweep_kernel, 32 * wpb, smem);
-  if (per_sm < 1) per_sm = 1;
-  u32 blocks = (u32)(device_sm_count() * per_sm);
-  const u32 need = (z.n_docs + wpb - 1) / wpb;
-  if (blocks > need) blocks = need;
-  z_sweep_kernel<<<blocks, 32 * wpb, smem, s>>>(a);
 }
 
 void launch_debug_philox(const u32* ctr, u32 n, u32 k0, u32 k1, u32* out, cudaStream_t s) {

@@ -26,6 +26,7 @@ struct ModelDev {
   u32* n;      // V*K counts, word-major
   u32* q;      // V*K fixed-point Phi (raw x between the two Phi kernels)
   u64* al;     // V*K alias entries
+  u64* csr;    // V*K per-word lists of (q << 32 | k) for q > 0, ascending k, nnz[w] used
   u64* A;      // V   dense mass per word
   u64* S;      // K   per-topic normalisers
   u32* nnz;    // V   nonzero x per word
@@ -37,6 +38,7 @@ struct ZLaunch {
   u32* z;
   const u32* d_len;
   const u32* d_idx;
+  const u32* order;  // processing order of the documents (longest first); may be null
   u32* K_d;       // may be null
   u32 n_docs;
   u64 n_tokens;
