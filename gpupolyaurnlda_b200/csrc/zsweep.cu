@@ -2,9 +2,10 @@
 // src/cu/topics.cu:36-105, with count_topics / compute_product_cumsum /
 // draw_wary_search / draw_alias from src/cu/topics.cuh:63-192).
 //
-// One warp per document; documents come from a global work counter.  The
-// document's topic counts m_d live in shared memory as 16-bit counts plus a
-// bitmap of nonzero topics.  Per token (after removing its current topic):
+// One warp per document; documents come from a global work counter (longest
+// first when an order is given).  The document's topic counts m_d live in
+// shared memory as a dense array of 16-bit counts plus the sorted list of its
+// nonzero topics.  Per token (after removing its current topic):
 //   B      = sum_k m_dk * q[w][k]      (u64, exact)
 //   sparse iff u0 * (alpha*A[w] + B) < B
 //   sparse: target = floor(u1 * B); topic = first k in ascending order whose
@@ -14,11 +15,12 @@
 // then the topic is added back and n[w][topic] incremented.
 //
 // B and the prefix run over the intersection of the document's topics and the
-// word's nonzero q.  The warp walks whichever side is smaller: the document's
-// bitmap (gathering q[w][k]) or the word's list of nonzero q (gathering m_dk
-// from shared memory).  Either way each lane owns a contiguous range in
-// ascending topic order, so lane order then position is ascending topic order
-// and, the masses being exact integers, both walks select the same topic.
+// word's nonzero q.  The warp walks whichever list is shorter: the document's
+// sorted topic list (gathering q[w][k]) or the word's list of nonzero q
+// (gathering m_dk from shared memory).  Either way lane l takes the l-th
+// contiguous chunk of an ascending list, so lane order then position is
+// ascending topic order and, the masses being exact integers, both walks
+// select the same topic.
 #include <algorithm>
 #include <cmath>
 
@@ -35,22 +37,62 @@ constexpr size_t kZMaxSmem = 200 * 1024;
 struct ZKernelArgs {
   ModelDev m;
   ZLaunch z;
-  u32 wpl;       // bitmap words per lane
   double lg_Ka;  // lgamma(K * alpha)
   double lg_a;   // lgamma(alpha)
 };
+
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// First index i in the sorted list tl[0..n) with tl[i] >= k (warp-cooperative).
+__device__ __forceinline__ u32 list_lower_bound(const uint16_t* tl, u32 n, u32 k, u32 lane) {
+  u32 lo = 0;
+  while (n > 32) {
+    const u32 step = (n + 31) >> 5;
+    const u32 idx = lo + lane * step;
+    const bool lt = lane * step < n && tl[idx] < k;
+    u32 c = __popc(__ballot_sync(kFullMask, lt));
+    if (c == 0) c = 1;
+    lo += (c - 1) * step;
+    n = min(step, n - (c - 1) * step);
+  }
+  const bool lt = lane < n && tl[lo + lane] < k;
+  return lo + __popc(__ballot_sync(kFullMask, lt));
+}
+
+// Removes tl[pos] from a list of n entries (warp-cooperative shift left).
+__device__ __forceinline__ void list_erase(uint16_t* tl, u32 n, u32 pos, u32 lane) {
+  for (u32 b = pos; b + 1 < n; b += 32) {
+    const u32 src = b + 1 + lane;
+    const uint16_t v = src < n ? tl[src] : 0;
+    __syncwarp();
+    if (src < n) tl[src - 1] = v;
+    __syncwarp();
+  }
+}
+
+// Inserts k at tl[pos] in a list of n entries (warp-cooperative shift right).
+__device__ __forceinline__ void list_insert(uint16_t* tl, u32 n, u32 pos, u32 k, u32 lane) {
+  for (u32 top = n; top > pos; top = top > pos + 32 ? top - 32 : pos) {
+    const u32 src = top - 1 - lane;
+    const bool act = lane < top - pos && lane < 32;
+    const uint16_t v = act ? tl[src] : 0;
+    __syncwarp();
+    if (act) tl[src + 1] = v;
+    __syncwarp();
+  }
+  if (lane == 0) tl[pos] = (uint16_t)k;
+  __syncwarp();
+}
 
 __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
   extern __shared__ __align__(16) unsigned char zsm[];
   const ModelDev& m = a.m;
   const ZLaunch& p = a.z;
   const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const u32 K = m.K, V = m.V, wpl = a.wpl;
+  const u32 K = m.K, V = m.V;
   const u32 Kp = (K + 63) & ~63u;
-  const u32 nbw = 32 * wpl;
-  const size_t per_warp = (size_t)Kp * 2 + (size_t)nbw * 4;
-  uint16_t* cnt = (uint16_t*)(zsm + warp * per_warp);
-  u32* bits = (u32*)(zsm + warp * per_warp + (size_t)Kp * 2);
+  uint16_t* cnt = (uint16_t*)(zsm + (size_t)warp * Kp * 4);
+  uint16_t* tl = cnt + Kp;  // sorted nonzero topics of the document
   const bool want_ll = (p.flags & 1u) && p.ll;
 
   u64 st_tok = 0, st_docs = 0, st_S = 0, st_sp = 0;
@@ -74,7 +116,6 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
       continue;
     }
     for (u32 i = lane; i < Kp / 8; i += 32) reinterpret_cast<uint4*>(cnt)[i] = make_uint4(0, 0, 0, 0);
-    for (u32 i = lane; i < nbw; i += 32) bits[i] = 0;
     __syncwarp();
     for (u32 i = lane; i < L; i += 32) {
       u32 k = p.z[off + i];
@@ -83,12 +124,27 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
         k %= K;
       }
       atomicAdd(reinterpret_cast<u32*>(cnt) + (k >> 1), 1u << ((k & 1) * 16));
-      atomicOr(bits + (k >> 5), 1u << (k & 31));
     }
     __syncwarp();
-    u32 nz = 0;  // distinct topics in the document (warp-uniform)
-    for (u32 b = 0; b < wpl; ++b) nz += __popc(bits[lane * wpl + b]);
-    nz = (u32)warp_sum_u64(nz);
+    // Sorted list of the nonzero topics: lane l compacts its contiguous range.
+    u32 nz;
+    {
+      const u32 per = Kp / 32;
+      const u32 k0 = lane * per;
+      u32 c = 0;
+      for (u32 k = k0; k < k0 + per; ++k) c += cnt[k] != 0;
+      u32 pos = c;
+#pragma unroll
+      for (u32 o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(kFullMask, pos, o);
+        if (lane >= o) pos += y;
+      }
+      nz = __shfl_sync(kFullMask, pos, 31);
+      pos -= c;
+      for (u32 k = k0; k < k0 + per; ++k)
+        if (cnt[k]) tl[pos++] = (uint16_t)k;
+      __syncwarp();
+    }
 
     for (u32 base = 0; base < L; base += 32) {
       const u32 i = base + lane;
@@ -120,46 +176,43 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
         const u64* __restrict__ crow = m.csr + row;
         const u32 nw = __shfl_sync(kFullMask, my_nw, j);
         const u64 Aw = __shfl_sync(kFullMask, my_A, j);
+        // remove the token's current topic
+        const u32 cz = cnt[zj];
+        __syncwarp();
+        if (lane == 0) cnt[zj] = (uint16_t)(cz - 1u);
+        if (cz == 1u) {
+          list_erase(tl, nz, list_lower_bound(tl, nz, zj, lane), lane);
+          --nz;
+        }
+        __syncwarp();
+        const bool word_side = nw < nz;
         if (j + 1 < nt) {
-          // Warm L1 with the next token's lines: this lane's q line and the
-          // start of its share of the word's nonzero list.
+          // Warm L1 with the next token's first line of this lane's share.
           const u32 wn = __shfl_sync(kFullMask, my_w, j + 1);
           const u32 nn = __shfl_sync(kFullMask, my_nw, j + 1);
           const size_t rn = (size_t)wn * K;
-          if (lane * wpl * 32 < K) asm volatile("prefetch.global.L1 [%0];" ::"l"(m.q + rn + lane * wpl * 32));
-          const u32 cn = (nn + 31) >> 5;
-          if (lane * cn < nn) asm volatile("prefetch.global.L1 [%0];" ::"l"(m.csr + rn + lane * cn));
-        }
-        u32 emptied = 0;
-        if (lane == 0) {
-          const u32 c = cnt[zj] - 1u;
-          cnt[zj] = (uint16_t)c;
-          if (c == 0) {
-            bits[zj >> 5] &= ~(1u << (zj & 31));
-            emptied = 1;
+          if (nn < nz) {
+            const u32 cn = (nn + 31) >> 5;
+            if (lane * cn < nn) prefetch_l1(m.csr + rn + lane * cn);
+          } else {
+            const u32 cd = (nz + 31) >> 5;
+            if (lane * cd < nz) prefetch_l1(m.q + rn + tl[lane * cd]);
           }
         }
-        nz -= __shfl_sync(kFullMask, emptied, 0);
-        __syncwarp();
-        // Sparse mass over this lane's contiguous range.
-        const bool word_side = nw < nz;
-        const u32 cper = (nw + 31) >> 5;
+        // Sparse mass over this lane's contiguous chunk.
+        const u32 len = word_side ? nw : nz;
+        const u32 cper = (len + 31) >> 5;
+        const u32 e0 = min(len, lane * cper), e1 = min(len, e0 + cper);
         u64 ls = 0;
         if (word_side) {
-          const u32 e0 = min(nw, lane * cper), e1 = min(nw, e0 + cper);
           for (u32 e = e0; e < e1; ++e) {
             const u64 ent = __ldg(crow + e);
             ls += (u64)cnt[(u32)ent & 0xffffu] * (u32)(ent >> 32);
           }
         } else {
-          for (u32 b = 0; b < wpl; ++b) {
-            const u32 wi = lane * wpl + b;
-            u32 bm = bits[wi];
-            while (bm) {
-              const u32 k = wi * 32 + (__ffs(bm) - 1);
-              bm &= bm - 1;
-              ls += (u64)cnt[k] * __ldg(qrow + k);
-            }
+          for (u32 e = e0; e < e1; ++e) {
+            const u32 k = tl[e];
+            ls += (u64)cnt[k] * __ldg(qrow + k);
           }
         }
         const u64 incl = warp_incl_scan_u64(ls, lane);
@@ -172,43 +225,30 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
             const u64 target = scale_u32(r1, B);
             const u32 f = __ffs(__ballot_sync(kFullMask, incl > target)) - 1;
             u64 run = __shfl_sync(kFullMask, incl - ls, f);
-            // Finish inside lane f's range, 32 candidates at a time.
-            if (word_side) {
-              const u32 e0 = min(nw, f * cper), e1 = min(nw, e0 + cper);
-              for (u32 s0 = e0; s0 < e1; s0 += 32) {
-                const u32 e = s0 + lane;
-                u64 mass = 0;
-                u32 kk = 0;
-                if (e < e1) {
+            // Finish inside lane f's chunk, 32 candidates at a time.
+            const u32 f0 = min(len, f * cper), f1 = min(len, f0 + cper);
+            for (u32 s0 = f0; s0 < f1; s0 += 32) {
+              const u32 e = s0 + lane;
+              u64 mass = 0;
+              u32 kk = 0;
+              if (e < f1) {
+                if (word_side) {
                   const u64 ent = __ldg(crow + e);
                   kk = (u32)ent & 0xffffu;
                   mass = (u64)cnt[kk] * (u32)(ent >> 32);
+                } else {
+                  kk = tl[e];
+                  mass = (u64)cnt[kk] * __ldg(qrow + kk);
                 }
-                const u64 in2 = warp_incl_scan_u64(mass, lane);
-                const u64 tot = __shfl_sync(kFullMask, in2, 31);
-                if (run + tot > target) {
-                  const u32 jj = __ffs(__ballot_sync(kFullMask, run + in2 > target)) - 1;
-                  k = __shfl_sync(kFullMask, kk, jj);
-                  break;
-                }
-                run += tot;
               }
-            } else {
-              for (u32 b = 0; b < wpl; ++b) {
-                const u32 wi = f * wpl + b;
-                const u32 bm = bits[wi];
-                const u32 kk = wi * 32 + lane;
-                u64 mass = 0;
-                if ((bm >> lane) & 1u) mass = (u64)cnt[kk] * __ldg(qrow + kk);
-                const u64 in2 = warp_incl_scan_u64(mass, lane);
-                const u64 tot = __shfl_sync(kFullMask, in2, 31);
-                if (run + tot > target) {
-                  const u32 jj = __ffs(__ballot_sync(kFullMask, run + in2 > target)) - 1;
-                  k = wi * 32 + jj;
-                  break;
-                }
-                run += tot;
+              const u64 in2 = warp_incl_scan_u64(mass, lane);
+              const u64 tot = __shfl_sync(kFullMask, in2, 31);
+              if (run + tot > target) {
+                const u32 jj = __ffs(__ballot_sync(kFullMask, run + in2 > target)) - 1;
+                k = __shfl_sync(kFullMask, kk, jj);
+                break;
               }
+              run += tot;
             }
           } else {
             const u32 r3 = __shfl_sync(kFullMask, r.w, j);
@@ -217,14 +257,11 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
             k = alias_pick(e, s, r3);
           }
         }
-        u32 filled = 0;
+        // add the new topic
+        const u32 ck = cnt[k];
+        __syncwarp();
         if (lane == 0) {
-          const u32 c = cnt[k] + 1u;
-          cnt[k] = (uint16_t)c;
-          if (c == 1) {
-            bits[k >> 5] |= 1u << (k & 31);
-            filled = 1;
-          }
+          cnt[k] = (uint16_t)(ck + 1u);
           atomicAdd(m.n + row + k, 1u);
           st_S += min(nz, nw);
           st_sp += (sp && !degenerate) ? 1 : 0;
@@ -236,7 +273,10 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
               ll_skip += 1.0;
           }
         }
-        nz += __shfl_sync(kFullMask, filled, 0);
+        if (ck == 0u) {
+          list_insert(tl, nz, list_lower_bound(tl, nz, k, lane), k, lane);
+          ++nz;
+        }
         if (lane == j) new_z = k;
         __syncwarp();
       }
@@ -245,15 +285,7 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
     if (lane == 0 && p.K_d) p.K_d[doc] = nz;
     if (want_ll) {
       double dl = 0.0;
-      for (u32 b = 0; b < wpl; ++b) {
-        const u32 wi = lane * wpl + b;
-        u32 bm = bits[wi];
-        while (bm) {
-          const u32 k = wi * 32 + (__ffs(bm) - 1);
-          bm &= bm - 1;
-          dl += lgamma((double)m.alpha + (double)cnt[k]) - a.lg_a;
-        }
-      }
+      for (u32 e = lane; e < nz; e += 32) dl += lgamma((double)m.alpha + (double)cnt[tl[e]]) - a.lg_a;
       dl = warp_sum_f64(dl);
       if (lane == 0) ll_acc += dl + a.lg_Ka - lgamma((double)K * (double)m.alpha + (double)L);
     }
@@ -279,9 +311,7 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
 
 size_t z_sweep_smem_per_warp(u32 K) {
   const u32 Kp = (K + 63) & ~63u;
-  const u32 nw = (K + 31) / 32;
-  const u32 wpl = (nw + 31) / 32;
-  return (size_t)Kp * 2 + (size_t)32 * wpl * 4;
+  return (size_t)Kp * 4;
 }
 
 void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s) {
@@ -289,8 +319,6 @@ void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s) {
   ZKernelArgs a;
   a.m = m;
   a.z = z;
-  const u32 nw = (m.K + 31) / 32;
-  a.wpl = (nw + 31) / 32;
   a.lg_a = std::lgamma((double)m.alpha);
   a.lg_Ka = std::lgamma((double)m.K * (double)m.alpha);
   const size_t per_warp = z_sweep_smem_per_warp(m.K);
