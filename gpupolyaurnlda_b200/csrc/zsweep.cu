@@ -41,7 +41,6 @@ struct ZKernelArgs {
   double lg_a;   // lgamma(alpha)
 };
 
-__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
 // First index i in the sorted list tl[0..n) with tl[i] >= k (warp-cooperative).
 __device__ __forceinline__ u32 list_lower_bound(const uint16_t* tl, u32 n, u32 k, u32 lane) {
@@ -59,15 +58,23 @@ __device__ __forceinline__ u32 list_lower_bound(const uint16_t* tl, u32 n, u32 k
   return lo + __popc(__ballot_sync(kFullMask, lt));
 }
 
-// Removes tl[pos] from a list of n entries (warp-cooperative shift left).
-__device__ __forceinline__ void list_erase(uint16_t* tl, u32 n, u32 pos, u32 lane) {
-  for (u32 b = pos; b + 1 < n; b += 32) {
-    const u32 src = b + 1 + lane;
-    const uint16_t v = src < n ? tl[src] : 0;
+// Drops the entries of topics whose count is zero from the list tl[0..n)
+// (stable, in place, warp-cooperative) and clears their in-list bits.
+// Returns the new length.
+__device__ __forceinline__ u32 list_compact(uint16_t* tl, u32 n, const uint16_t* cnt, u32* inl, u32 lane) {
+  u32 out = 0;
+  for (u32 b = 0; b < n; b += 32) {
+    const u32 e = b + lane;
+    const u32 k = e < n ? tl[e] : 0u;
+    const bool keep = e < n && cnt[k] != 0;
+    const u32 ball = __ballot_sync(kFullMask, keep);
     __syncwarp();
-    if (src < n) tl[src - 1] = v;
+    if (keep) tl[out + __popc(ball & ((1u << lane) - 1u))] = (uint16_t)k;
+    if (e < n && !keep) atomicAnd(inl + (k >> 5), ~(1u << (k & 31)));
+    out += __popc(ball);
     __syncwarp();
   }
+  return out;
 }
 
 // Inserts k at tl[pos] in a list of n entries (warp-cooperative shift right).
@@ -84,6 +91,12 @@ __device__ __forceinline__ void list_insert(uint16_t* tl, u32 n, u32 pos, u32 k,
   __syncwarp();
 }
 
+// Shared memory per warp: counts and list (2 x Kp u16) and the in-list bitmap.
+__host__ __device__ __forceinline__ size_t z_warp_bytes(u32 K) {
+  const size_t Kp = (K + 63) & ~63u;
+  return Kp * 4 + ((Kp / 8 + 15) & ~(size_t)15);
+}
+
 __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
   extern __shared__ __align__(16) unsigned char zsm[];
   const ModelDev& m = a.m;
@@ -91,8 +104,12 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
   const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const u32 K = m.K, V = m.V;
   const u32 Kp = (K + 63) & ~63u;
-  uint16_t* cnt = (uint16_t*)(zsm + (size_t)warp * Kp * 4);
-  uint16_t* tl = cnt + Kp;  // sorted nonzero topics of the document
+  uint16_t* cnt = (uint16_t*)(zsm + (size_t)warp * z_warp_bytes(K));
+  // Sorted topics of the document: every topic with a nonzero count, plus
+  // topics whose count fell to zero since the last compaction (their mass is
+  // zero, so they never change B or the selected topic).
+  uint16_t* tl = cnt + Kp;
+  u32* inl = (u32*)(tl + Kp);  // bitmap: topic is in tl
   const bool want_ll = (p.flags & 1u) && p.ll;
 
   u64 st_tok = 0, st_docs = 0, st_S = 0, st_sp = 0;
@@ -116,6 +133,7 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
       continue;
     }
     for (u32 i = lane; i < Kp / 8; i += 32) reinterpret_cast<uint4*>(cnt)[i] = make_uint4(0, 0, 0, 0);
+    for (u32 i = lane; i < Kp / 32; i += 32) inl[i] = 0;
     __syncwarp();
     for (u32 i = lane; i < L; i += 32) {
       u32 k = p.z[off + i];
@@ -142,9 +160,13 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
       nz = __shfl_sync(kFullMask, pos, 31);
       pos -= c;
       for (u32 k = k0; k < k0 + per; ++k)
-        if (cnt[k]) tl[pos++] = (uint16_t)k;
+        if (cnt[k]) {
+          tl[pos++] = (uint16_t)k;
+          atomicOr(inl + (k >> 5), 1u << (k & 31));
+        }
       __syncwarp();
     }
+    u32 nl = nz;  // list length (nz plus dead entries)
 
     for (u32 base = 0; base < L; base += 32) {
       const u32 i = base + lane;
@@ -180,27 +202,11 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
         const u32 cz = cnt[zj];
         __syncwarp();
         if (lane == 0) cnt[zj] = (uint16_t)(cz - 1u);
-        if (cz == 1u) {
-          list_erase(tl, nz, list_lower_bound(tl, nz, zj, lane), lane);
-          --nz;
-        }
+        if (cz == 1u) --nz;  // the entry stays in the list until compaction
         __syncwarp();
-        const bool word_side = nw < nz;
-        if (j + 1 < nt) {
-          // Warm L1 with the next token's first line of this lane's share.
-          const u32 wn = __shfl_sync(kFullMask, my_w, j + 1);
-          const u32 nn = __shfl_sync(kFullMask, my_nw, j + 1);
-          const size_t rn = (size_t)wn * K;
-          if (nn < nz) {
-            const u32 cn = (nn + 31) >> 5;
-            if (lane * cn < nn) prefetch_l1(m.csr + rn + lane * cn);
-          } else {
-            const u32 cd = (nz + 31) >> 5;
-            if (lane * cd < nz) prefetch_l1(m.q + rn + tl[lane * cd]);
-          }
-        }
+        const bool word_side = nw < nl;
         // Sparse mass over this lane's contiguous chunk.
-        const u32 len = word_side ? nw : nz;
+        const u32 len = word_side ? nw : nl;
         const u32 cper = (len + 31) >> 5;
         const u32 e0 = min(len, lane * cper), e1 = min(len, e0 + cper);
         u64 ls = 0;
@@ -274,9 +280,15 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
           }
         }
         if (ck == 0u) {
-          list_insert(tl, nz, list_lower_bound(tl, nz, k, lane), k, lane);
           ++nz;
+          if (!((inl[k >> 5] >> (k & 31)) & 1u)) {
+            list_insert(tl, nl, list_lower_bound(tl, nl, k, lane), k, lane);
+            if (lane == 0) atomicOr(inl + (k >> 5), 1u << (k & 31));
+            __syncwarp();
+            ++nl;
+          }
         }
+        if (nl - nz > 32u) nl = list_compact(tl, nl, cnt, inl, lane);
         if (lane == j) new_z = k;
         __syncwarp();
       }
@@ -285,7 +297,10 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
     if (lane == 0 && p.K_d) p.K_d[doc] = nz;
     if (want_ll) {
       double dl = 0.0;
-      for (u32 e = lane; e < nz; e += 32) dl += lgamma((double)m.alpha + (double)cnt[tl[e]]) - a.lg_a;
+      for (u32 e = lane; e < nl; e += 32) {
+        const u32 c = cnt[tl[e]];
+        if (c) dl += lgamma((double)m.alpha + (double)c) - a.lg_a;
+      }
       dl = warp_sum_f64(dl);
       if (lane == 0) ll_acc += dl + a.lg_Ka - lgamma((double)K * (double)m.alpha + (double)L);
     }
@@ -309,10 +324,7 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
 
 }  // namespace
 
-size_t z_sweep_smem_per_warp(u32 K) {
-  const u32 Kp = (K + 63) & ~63u;
-  return (size_t)Kp * 4;
-}
+size_t z_sweep_smem_per_warp(u32 K) { return z_warp_bytes(K); }
 
 void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s) {
   if (!z.n_docs) return;
