@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--docs", type=int, default=None, help="override the number of documents")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the baseline sample")
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU seconds per timed oracle iteration")
     return p.parse_args()
 
 
@@ -108,6 +108,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, device) -> float:
+    """Max of a per-rank timing over all ranks (identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(n_tokens: int, steps: int, world: int, seconds_max: float) -> float:
+    """Whole-job tokens/s of `world` independent chains (one per GPU, each over
+    the full corpus): every rank sweeps n_tokens per step; the job takes the
+    slowest rank's time."""
+    return world * n_tokens * steps / seconds_max
+
+
 def make_corpus(args, device):
     from gpupolyaurnlda_b200 import corpus
     return corpus.generate(args.workload, seed=1, device=device, D=args.docs)
@@ -120,36 +137,60 @@ def workload_desc(c, args):
             "l2": "inputs larger than L2 (fixed-point Phi 4KV B, alias tables 8KV B, corpus 8N B)"}
 
 
-def cpu_baseline(c, seconds: float, threads: int | None = None):
-    """One Phi step over all K*V cells plus a z sweep over a leading slice of the
-    documents sized for ~`seconds` of work, extrapolated to a full iteration."""
-    import oracle
-    threads = threads or oracle.default_threads()
-    ch = oracle.Chain(c.K, c.alpha, c.beta, c.counts, seed=0, threads=threads)
-    t0 = time.perf_counter()
-    ch.sample_phi()
-    t_phi = time.perf_counter() - t0
-    # probe speed on a small slice, then size the sample
-    cum = np.cumsum(c.d_len.astype(np.int64))
-    probe_docs = int(np.searchsorted(cum, min(c.n_tokens, 200000))) + 1
-    probe_docs = min(probe_docs, c.n_docs)
-    ntok = int(cum[probe_docs - 1])
-    z = c.z[:ntok].copy()
-    t0 = time.perf_counter()
-    ch.sweep(c.w[:ntok], z, c.d_len[:probe_docs])
-    rate = ntok / max(1e-9, time.perf_counter() - t0)
-    want = int(min(c.n_tokens, max(ntok, rate * max(1.0, seconds - t_phi))))
-    docs = min(c.n_docs, int(np.searchsorted(cum, want)) + 1)
-    ntok = int(cum[docs - 1])
-    z = c.z[:ntok].copy()
-    ch.tok_base = 0
-    t0 = time.perf_counter()
-    ch.sweep(c.w[:ntok], z, c.d_len[:docs])
-    t_z = time.perf_counter() - t0
-    t_iter = t_phi + t_z * (c.n_tokens / ntok)
-    return {"value": c.n_tokens / t_iter, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"one Phi step over all {c.K}x{c.V} cells ({t_phi:.2f} s) + z sweep over the first {docs} "
-                      f"documents ({ntok} tokens, {t_z:.2f} s), extrapolated to {c.n_tokens} tokens"}
+class CpuChain:
+    """The CPU oracle's sweep (same algorithm and random streams) on a leading
+    slice of the documents, sized so one iteration takes about `seconds`.
+    Each step is one full iteration of that chain: the Phi step over all K*V
+    cells and a z sweep over the slice; tokens/s is extrapolated to the whole
+    corpus as N / (t_phi + t_z * N / n_slice)."""
+
+    def __init__(self, c, seconds: float, threads: int | None = None):
+        import oracle
+        self.c = c
+        self.threads = threads or oracle.default_threads()
+        self.ch = oracle.Chain(c.K, c.alpha, c.beta, c.counts, seed=0, threads=self.threads)
+        cum = np.cumsum(c.d_len.astype(np.int64))
+        # probe: one Phi step and a sweep of ~2e5 tokens
+        t0 = time.perf_counter()
+        self.ch.sample_phi()
+        t_phi = time.perf_counter() - t0
+        pd = min(c.n_docs, int(np.searchsorted(cum, min(c.n_tokens, 200000))) + 1)
+        pt = int(cum[pd - 1])
+        t0 = time.perf_counter()
+        self.ch.sweep(c.w[:pt], c.z[:pt].copy(), c.d_len[:pd])
+        rate = pt / max(1e-9, time.perf_counter() - t0)
+        want = int(min(c.n_tokens, max(pt, rate * max(1.0, seconds - t_phi))))
+        self.docs = min(c.n_docs, int(np.searchsorted(cum, want)) + 1)
+        self.ntok = int(cum[self.docs - 1])
+        self.z = c.z[:self.ntok].copy()
+        self.ch = oracle.Chain(c.K, c.alpha, c.beta, c.counts, seed=0, threads=self.threads)
+        self.last = None
+
+    def step(self) -> float:
+        t0 = time.perf_counter()
+        self.ch.sample_phi()
+        t_phi = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        self.ch.sweep(self.c.w[:self.ntok], self.z, self.c.d_len[:self.docs])
+        t_z = time.perf_counter() - t0
+        self.last = (t_phi, t_z)
+        return self.c.n_tokens / (t_phi + t_z * (self.c.n_tokens / self.ntok))
+
+    def describe(self, value: float, warm: int) -> dict:
+        t_phi, t_z = self.last
+        return {"value": value, "unit": UNIT, "cores": self.threads, "kind": "port",
+                "sample": f"CPU oracle chain on the first {self.docs} documents ({self.ntok} of {self.c.n_tokens} "
+                          f"tokens) after {warm} warm-up iterations; per iteration a Phi step over all "
+                          f"{self.c.K}x{self.c.V} cells ({t_phi:.2f} s) and a z sweep of the slice ({t_z:.2f} s), "
+                          f"extrapolated to the whole corpus"}
+
+
+def cpu_baseline(c, seconds: float, warm: int = 2):
+    cc = CpuChain(c, seconds)
+    for _ in range(warm):
+        cc.step()
+    v = cc.step()
+    return cc.describe(v, warm)
 
 
 def run_reference(args):
@@ -158,21 +199,22 @@ def run_reference(args):
         return
     dev = "cuda" if _cuda() else "cpu"
     c = make_corpus(args, dev)
+    cc = CpuChain(c, args.cpu_seconds)
     vals = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(c, args.cpu_seconds)
+        v = cc.step()
         if i >= args.warmup:
-            vals.append(r["value"])
+            vals.append(v)
     v = float(np.median(vals))
     ms = c.n_tokens / v * 1e3
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
             "config": dict(workload_desc(c, args), parallelism="cpu"),
-            "cpu_baseline": dict(r, value=v),
+            "cpu_baseline": cc.describe(v, args.warmup),
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "CPU oracle port of the sweep (the reference has no CPU implementation; its CUDA kernels are "
-                    "not run on this pool)"}
+            "note": "CPU oracle port of the sweep (the reference has no CPU implementation of the path; its CUDA "
+                    "kernels are not run on this pool)"}
     print(json.dumps(line), flush=True)
 
 
@@ -228,16 +270,13 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    ms_max = max_over_ranks(e0.elapsed_time(e1), f"cuda:{local}")
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    ms_max = float(t.item())
     s.set_stream(0)
     s.close()
 
-    value = world * c.n_tokens * args.steps / (ms_max / 1e3)
+    value = replica_value(c.n_tokens, args.steps, world, ms_max / 1e3)
     zb = [24 * c.n_tokens + 8 * c.n_docs + 4 * S for S in S_work]
     z_gbs = float(np.mean([b / (m / 1e3) / 1e9 for b, m in zip(zb, z_ms)]))
     B_iter = [20 * c.K * c.V + b for b in zb]
@@ -261,18 +300,15 @@ def run_ours(args):
         for _ in range(args.steps):
             s.sample_phi()
             s.sweep_buffer(0, zn, wn, dn, kn)
-        el = time.perf_counter() - t0
+        el = max_over_ranks(time.perf_counter() - t0, f"cuda:{local}")
         s.close()
-        te = torch.tensor([el], dtype=torch.float64, device=f"cuda:{local}")
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * c.n_tokens * args.steps / float(te.item()), "unit": UNIT,
+        e2e = {"value": replica_value(c.n_tokens, args.steps, world, el), "unit": UNIT,
                "h2d_bytes_per_step": 8 * c.n_tokens + 8 * c.n_docs, "d2h_bytes_per_step": 4 * c.n_tokens,
                "path": "initialize/sample_phi/sample_z_async/sync_buffer, one buffer per iteration, pinned host"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(c, args.cpu_seconds)
+        cpu = cpu_baseline(c, args.cpu_seconds / 3, warm=2)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
