@@ -125,6 +125,16 @@ def replica_value(n_tokens: int, steps: int, world: int, seconds_max: float) -> 
     return world * n_tokens * steps / seconds_max
 
 
+def measured_traffic_per_token():
+    """DRAM bytes per token of the z-sweep kernel from the committed ncu
+    summary (a smaller case of the same workload; traffic scales with tokens)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "z_sweep_kernel_traffic.json")) as f:
+            return float(json.load(f)["dram_bytes_per_token"])
+    except Exception:
+        return None
+
+
 def make_corpus(args, device):
     from gpupolyaurnlda_b200 import corpus
     return corpus.generate(args.workload, seed=1, device=device, D=args.docs)
@@ -317,7 +327,10 @@ def run_ours(args):
                 "config": dict(workload_desc(c, args),
                                parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
                 "roofline": {"bound": "hbm", "achieved": z_gbs, "peak": hbm, "unit": "GB/s",
-                             "frac": z_gbs / hbm, "traffic": None, "kernel": "z_sweep_kernel",
+                             "frac": z_gbs / hbm,
+                             "traffic": (tpt * c.n_tokens if (tpt := measured_traffic_per_token()) else None),
+                             "traffic_note": "ncu dram bytes per token of a 3.4e7-token slice, scaled to N",
+                             "kernel": "z_sweep_kernel",
                              "algorithmic_bytes_per_launch": float(np.mean(zb)), "peak_kind": peak_kind},
                 "iteration_roofline": {"achieved": it_gbs, "frac": it_gbs / hbm,
                                        "bytes_per_iteration": float(np.mean(B_iter))},
