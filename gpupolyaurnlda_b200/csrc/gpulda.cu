@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -31,9 +32,16 @@ namespace {
 
 enum TimerSlot { kTPhi = 0, kTPrep = 1, kTAlias = 2, kTOffsets = 3, kTZ = 4, kTN = 5 };
 
+// A buffer's sweep is split into this many pieces of about equal token counts
+// so that copying piece p+1 in and piece p-1 out overlaps sweeping piece p.
+constexpr u32 kPieces = 8;
+
 struct BufCtx {
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  cudaStream_t stream = nullptr;  // sweeps
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaStream_t piece[kPieces] = {};  // one stream per piece, so piece sweeps overlap
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // [0] order copied, [1] last copy out issued
+  cudaEvent_t in[kPieces] = {}, out[kPieces] = {};
   bool used = false;
   u32* order = nullptr;           // device: document processing order
   std::vector<u32> order_host;    // host staging of the order
@@ -221,7 +229,7 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
       (rc = dalloc(&g.dev.A, g.V)) || (rc = dalloc(&g.dev.S, g.K)) || (rc = dalloc(&g.dev.nnz, g.V)) ||
       (rc = dalloc(&g.C, g.V)) || (rc = dalloc(&g.cdf, (size_t)kPoisN * kPoisW)) ||
       (rc = dalloc(&g.guide, (size_t)kPoisN * 256)) || (rc = dalloc(&g.lfac, kLogFacN)) ||
-      (rc = dalloc(&g.counters, kCtrN)) || (rc = dalloc(&g.ll, 2)) || (rc = dalloc(&g.work, 1)) ||
+      (rc = dalloc(&g.counters, kCtrN)) || (rc = dalloc(&g.ll, 2)) || (rc = dalloc(&g.work, 1 + kPieces)) ||
       (rc = dalloc(&g.status, 1))) {
     free_model();
     return rc;
@@ -256,7 +264,14 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
     Buffer& b = buffers[i];
     BufCtx* ctx = new BufCtx();
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
+    CK(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
+    for (auto& ps : ctx->piece) CK(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
+    for (auto& e : ctx->ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (u32 i = 0; i < kPieces; ++i) {
+      CK(cudaEventCreateWithFlags(&ctx->in[i], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&ctx->out[i], cudaEventDisableTiming));
+    }
     cudaStream_t* sp = new cudaStream_t(ctx->stream);
     b.stream = sp;
     b.gpu_rng = ctx;
@@ -301,16 +316,12 @@ int phi_step_async(cudaStream_t s) {
 }
 
 // One sweep over documents already on the device.
-int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_idx, const u32* order, u32* K_d,
-                 u32 n_docs, u64 n_tokens, bool offsets, cudaEvent_t* ev) {
-  CK(cudaEventRecord(ev[0], s));
-  if (offsets) {
-    launch_doc_offsets(d_len, d_idx, n_docs, s);
-    CK(cudaGetLastError());
-    g.launches += 1;
-  }
-  CK(cudaEventRecord(ev[1], s));
-  CK(cudaMemsetAsync(g.work, 0, 4, s));
+// One z-sweep launch over n_docs documents whose d_len / d_idx / order / K_d
+// start at the given pointers; d_idx offsets are relative to z and w, and the
+// tokens' Philox indices start at tok_base.
+int z_launch(cudaStream_t s, u32* z, const u32* w, const u32* d_len, const u32* d_idx, const u32* order, u32* K_d,
+             u32 n_docs, u64 n_tokens, u64 tok_base, u32* work) {
+  CK(cudaMemsetAsync(work, 0, 4, s));
   ZLaunch zl;
   zl.w = w;
   zl.z = z;
@@ -320,19 +331,113 @@ int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_
   zl.K_d = K_d;
   zl.n_docs = n_docs;
   zl.n_tokens = n_tokens;
-  zl.tok_base = g.tok_offset;
+  zl.tok_base = tok_base;
   zl.t = (u32)g.t;
   zl.flags = (g.flags & GPULDA_FLAG_LOGLIK) ? 1u : 0u;
   zl.counters = g.counters;
   zl.ll = g.ll;
-  zl.work = g.work;
+  zl.work = work;
   zl.status = g.status;
   launch_z_sweep(g.dev, zl, s);
   CK(cudaGetLastError());
-  CK(cudaEventRecord(ev[2], s));
   g.launches += 1;
+  return GPULDA_OK;
+}
+
+int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_idx, const u32* order, u32* K_d,
+                 u32 n_docs, u64 n_tokens, bool offsets, cudaEvent_t* ev) {
+  CK(cudaEventRecord(ev[0], s));
+  if (offsets) {
+    launch_doc_offsets(d_len, d_idx, n_docs, s);
+    CK(cudaGetLastError());
+    g.launches += 1;
+  }
+  CK(cudaEventRecord(ev[1], s));
+  int rc = z_launch(s, z, w, d_len, d_idx, order, K_d, n_docs, n_tokens, g.tok_offset, g.work);
+  if (rc) return rc;
+  CK(cudaEventRecord(ev[2], s));
   g.tok_offset += n_tokens;
   g.swept = true;
+  return GPULDA_OK;
+}
+
+// sample_z_async for host buffers: kPieces pieces of whole documents with
+// about equal token counts; piece p's tokens are copied in on the h2d stream,
+// swept on the buffer's stream once they have arrived, and copied out on the
+// d2h stream once swept.  Token numbering stays buffer-relative, so the result
+// does not depend on the split.
+int pipelined_sweep(Buffer* b, BufCtx* ctx) {
+  const u32 n = b->n_docs;
+  const size_t db = (size_t)n * 4;
+  cudaStream_t s = ctx->stream;
+  u32 dcut[kPieces + 1];
+  u64 tcut[kPieces + 1];
+  dcut[0] = 0;
+  tcut[0] = 0;
+  u64 cum = 0;
+  u32 pc = 1;
+  for (u32 i = 0; i < n && pc < kPieces; ++i) {
+    cum += b->d[i];
+    while (pc < kPieces && cum * kPieces >= (u64)b->n_tokens * pc) {
+      dcut[pc] = i + 1;
+      tcut[pc] = std::min<u64>(cum, b->n_tokens);
+      ++pc;
+    }
+  }
+  for (; pc <= kPieces; ++pc) {
+    dcut[pc] = n;
+    tcut[pc] = b->n_tokens;
+  }
+  if (ctx->used) CK(cudaEventSynchronize(ctx->ev[0]));
+  ctx->order_host.resize(n);
+  std::vector<u32> part;
+  for (u32 p = 0; p < kPieces; ++p) {
+    longest_first(b->d + dcut[p], dcut[p + 1] - dcut[p], part);
+    std::copy(part.begin(), part.end(), ctx->order_host.begin() + dcut[p]);
+  }
+  u32* gz = (u32*)b->gpu_z;
+  u32* gw = (u32*)b->gpu_w;
+  u32* gdl = (u32*)b->gpu_d_len;
+  u32* gdi = (u32*)b->gpu_d_idx;
+  u32* gkd = (u32*)b->gpu_K_d;
+  CK(cudaMemcpyAsync(gdl, b->d, db, cudaMemcpyHostToDevice, s));
+  if (b->K_d) CK(cudaMemcpyAsync(gkd, b->K_d, db, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->order, ctx->order_host.data(), db, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(ctx->ev[0], s));
+  CK(cudaEventRecord(g.z_ev[0], s));
+  launch_doc_offsets(gdl, gdi, n, s);
+  CK(cudaGetLastError());
+  g.launches += 1;
+  CK(cudaEventRecord(g.z_ev[1], s));
+  if (ctx->used) CK(cudaStreamWaitEvent(ctx->h2d, ctx->ev[1], 0));  // the previous copy out has read gpu_z
+  const u64 tok_base = g.tok_offset;
+  for (u32 p = 0; p < kPieces; ++p) {
+    const u64 t0 = tcut[p], t1 = tcut[p + 1];
+    if (t1 > t0) {
+      CK(cudaMemcpyAsync(gz + t0, b->z + t0, (t1 - t0) * 4, cudaMemcpyHostToDevice, ctx->h2d));
+      CK(cudaMemcpyAsync(gw + t0, b->w + t0, (t1 - t0) * 4, cudaMemcpyHostToDevice, ctx->h2d));
+    }
+    CK(cudaEventRecord(ctx->in[p], ctx->h2d));
+    cudaStream_t ps = ctx->piece[p];
+    CK(cudaStreamWaitEvent(ps, ctx->in[p], 0));
+    CK(cudaStreamWaitEvent(ps, g.z_ev[1], 0));  // document offsets are ready
+    const u32 nd = dcut[p + 1] - dcut[p];
+    if (nd) {
+      const int rc = z_launch(ps, gz, gw, gdl + dcut[p], gdi + dcut[p], ctx->order + dcut[p], gkd + dcut[p], nd,
+                              b->n_tokens, tok_base, g.work + 1 + p);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(ctx->out[p], ps));
+    CK(cudaStreamWaitEvent(s, ctx->out[p], 0));
+    CK(cudaStreamWaitEvent(ctx->d2h, ctx->out[p], 0));
+    if (t1 > t0) CK(cudaMemcpyAsync(b->z + t0, gz + t0, (t1 - t0) * 4, cudaMemcpyDeviceToHost, ctx->d2h));
+  }
+  CK(cudaEventRecord(g.z_ev[2], s));
+  CK(cudaEventRecord(ctx->ev[1], ctx->d2h));
+  g.tok_offset += b->n_tokens;
+  g.swept = true;
+  g.z_timed = true;
+  ctx->used = true;
   return GPULDA_OK;
 }
 
@@ -379,6 +484,10 @@ extern "C" void sample_z_async(Buffer* b) {
     return;
   }
   BufCtx* ctx = (BufCtx*)b->gpu_rng;
+  if (!g.user_stream && b->n_docs >= 4 * kPieces) {
+    pipelined_sweep(b, ctx);
+    return;
+  }
   cudaStream_t s = g.user_stream ? g.user_stream : ctx->stream;
   const size_t tb = (size_t)b->n_tokens * 4, db = (size_t)b->n_docs * 4;
 #define CKV(expr)                          \
@@ -415,6 +524,7 @@ extern "C" void sync_buffer(Buffer* b) {
   BufCtx* ctx = (BufCtx*)b->gpu_rng;
   cudaStream_t s = g.user_stream ? g.user_stream : ctx->stream;
   cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->d2h);
   if (e != cudaSuccess) {
     cuda_fail(e, "sync_buffer");
     return;
@@ -439,7 +549,15 @@ extern "C" void cleanup(Buffer* buffers, uint32_t n_buffers) {
       BufCtx* ctx = (BufCtx*)b.gpu_rng;
       for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+      for (u32 k = 0; k < kPieces; ++k) {
+        if (ctx->in[k]) cudaEventDestroy(ctx->in[k]);
+        if (ctx->out[k]) cudaEventDestroy(ctx->out[k]);
+      }
       if (ctx->stream) cudaStreamDestroy(ctx->stream);
+      if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
+      if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
+      for (auto& ps : ctx->piece)
+        if (ps) cudaStreamDestroy(ps);
       dfree(ctx->order);
       delete ctx;
     }
