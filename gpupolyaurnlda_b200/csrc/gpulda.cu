@@ -61,6 +61,36 @@ void longest_first(const u32* d_len, u32 n, std::vector<u32>& order) {
   for (u32 i = 0; i < n; ++i) order[start[max_len - d_len[i]]++] = i;
 }
 
+// Above this many topics a document's counts live in a shared-memory hash map
+// (a dense per-document count array would cost 2 K bytes of shared memory per
+// warp); documents of at most kShortDoc tokens are swept by one launch with a
+// small map per warp, longer ones by a second launch sized for the longest.
+constexpr u32 kMapMinK = 2048;
+constexpr u32 kShortDoc = 256;
+
+// Longest-first order with the short documents (length <= kShortDoc) first:
+// returns their count and the longest length among the rest.
+struct DocSplit {
+  u32 n_short = 0;
+  u32 lmax_long = 0;
+};
+
+DocSplit split_longest_first(const u32* d_len, u32 n, std::vector<u32>& order, u32 K) {
+  longest_first(d_len, n, order);
+  DocSplit sp;
+  if (K <= kMapMinK) return sp;
+  u32 first_short = n;
+  for (u32 i = 0; i < n; ++i)
+    if (d_len[order[i]] <= kShortDoc) {
+      first_short = i;
+      break;
+    }
+  sp.n_short = n - first_short;
+  sp.lmax_long = first_short > 0 ? d_len[order[0]] : 0;
+  std::rotate(order.begin(), order.begin() + first_short, order.end());
+  return sp;
+}
+
 struct Model {
   bool live = false;
   int fatal = 1;
@@ -86,6 +116,8 @@ struct Model {
   size_t alias_scratch_bytes = 0;
 
   cudaStream_t stream = nullptr;       // library stream
+  cudaStream_t side = nullptr;         // second stream for concurrent sweeps
+  cudaEvent_t fork = nullptr, join = nullptr;
   cudaStream_t user_stream = nullptr;  // caller-supplied stream, if any
   cudaEvent_t ev[6] = {};
   bool phi_timed = false, z_timed = false;
@@ -96,6 +128,7 @@ struct Model {
   u32 *cz = nullptr, *cw = nullptr, *cd_len = nullptr, *cd_idx = nullptr, *cK_d = nullptr, *corder = nullptr;
   u32 c_docs = 0;
   u64 c_tokens = 0;
+  DocSplit c_split;
 };
 
 Model g;
@@ -187,6 +220,9 @@ void free_model() {
   for (auto& e : g.z_ev)
     if (e) cudaEventDestroy(e);
   if (g.stream) cudaStreamDestroy(g.stream);
+  if (g.side) cudaStreamDestroy(g.side);
+  if (g.fork) cudaEventDestroy(g.fork);
+  if (g.join) cudaEventDestroy(g.join);
   const int fatal = g.fatal;
   g = Model();
   g.fatal = fatal;
@@ -222,6 +258,9 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
   const size_t cells = (size_t)g.K * g.V;
 
   CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&g.fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming));
   for (auto& e : g.ev) CK(cudaEventCreate(&e));
   for (auto& e : g.z_ev) CK(cudaEventCreate(&e));
   if ((rc = dalloc(&g.dev.n, cells)) || (rc = dalloc(&g.dev.q, cells)) || (rc = dalloc(&g.dev.al, cells)) ||
@@ -229,7 +268,7 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
       (rc = dalloc(&g.dev.A, g.V)) || (rc = dalloc(&g.dev.S, g.K)) || (rc = dalloc(&g.dev.nnz, g.V)) ||
       (rc = dalloc(&g.C, g.V)) || (rc = dalloc(&g.cdf, (size_t)kPoisN * kPoisW)) ||
       (rc = dalloc(&g.guide, (size_t)kPoisN * 256)) || (rc = dalloc(&g.lfac, kLogFacN)) ||
-      (rc = dalloc(&g.counters, kCtrN)) || (rc = dalloc(&g.ll, 2)) || (rc = dalloc(&g.work, 1 + kPieces)) ||
+      (rc = dalloc(&g.counters, kCtrN)) || (rc = dalloc(&g.ll, 2)) || (rc = dalloc(&g.work, 2 + kPieces)) ||
       (rc = dalloc(&g.status, 1))) {
     free_model();
     return rc;
@@ -320,7 +359,7 @@ int phi_step_async(cudaStream_t s) {
 // start at the given pointers; d_idx offsets are relative to z and w, and the
 // tokens' Philox indices start at tok_base.
 int z_launch(cudaStream_t s, u32* z, const u32* w, const u32* d_len, const u32* d_idx, const u32* order, u32* K_d,
-             u32 n_docs, u64 n_tokens, u64 tok_base, u32* work) {
+             u32 n_docs, u64 n_tokens, u64 tok_base, u32* work, u32 lmax = 0) {
   CK(cudaMemsetAsync(work, 0, 4, s));
   ZLaunch zl;
   zl.w = w;
@@ -338,14 +377,15 @@ int z_launch(cudaStream_t s, u32* z, const u32* w, const u32* d_len, const u32* 
   zl.ll = g.ll;
   zl.work = work;
   zl.status = g.status;
-  launch_z_sweep(g.dev, zl, s);
+  if (!(g.K > kMapMinK && lmax && launch_z_sweep_map(g.dev, zl, s, lmax))) launch_z_sweep(g.dev, zl, s);
   CK(cudaGetLastError());
   g.launches += 1;
   return GPULDA_OK;
 }
 
+// With a split (large K), `order` lists the short documents first.
 int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_idx, const u32* order, u32* K_d,
-                 u32 n_docs, u64 n_tokens, bool offsets, cudaEvent_t* ev) {
+                 u32 n_docs, u64 n_tokens, bool offsets, cudaEvent_t* ev, const DocSplit* split = nullptr) {
   CK(cudaEventRecord(ev[0], s));
   if (offsets) {
     launch_doc_offsets(d_len, d_idx, n_docs, s);
@@ -353,7 +393,22 @@ int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_
     g.launches += 1;
   }
   CK(cudaEventRecord(ev[1], s));
-  int rc = z_launch(s, z, w, d_len, d_idx, order, K_d, n_docs, n_tokens, g.tok_offset, g.work);
+  int rc = GPULDA_OK;
+  if (split && g.K > kMapMinK) {
+    // long documents on `s`, short ones concurrently on the side stream
+    CK(cudaEventRecord(g.fork, s));
+    CK(cudaStreamWaitEvent(g.side, g.fork, 0));
+    if (n_docs > split->n_short)
+      rc = z_launch(s, z, w, d_len, d_idx, order + split->n_short, K_d, n_docs - split->n_short, n_tokens,
+                    g.tok_offset, g.work, split->lmax_long);
+    if (!rc && split->n_short)
+      rc = z_launch(g.side, z, w, d_len, d_idx, order, K_d, split->n_short, n_tokens, g.tok_offset,
+                    g.work + 1 + kPieces, kShortDoc);
+    CK(cudaEventRecord(g.join, g.side));
+    CK(cudaStreamWaitEvent(s, g.join, 0));
+  } else {
+    rc = z_launch(s, z, w, d_len, d_idx, order, K_d, n_docs, n_tokens, g.tok_offset, g.work);
+  }
   if (rc) return rc;
   CK(cudaEventRecord(ev[2], s));
   g.tok_offset += n_tokens;
@@ -484,7 +539,7 @@ extern "C" void sample_z_async(Buffer* b) {
     return;
   }
   BufCtx* ctx = (BufCtx*)b->gpu_rng;
-  if (!g.user_stream && b->n_docs >= 4 * kPieces) {
+  if (!g.user_stream && b->n_docs >= 4 * kPieces && g.K <= kMapMinK) {
     pipelined_sweep(b, ctx);
     return;
   }
@@ -504,11 +559,11 @@ extern "C" void sample_z_async(Buffer* b) {
   if (b->K_d) CKV(cudaMemcpyAsync(b->gpu_K_d, b->K_d, db, cudaMemcpyHostToDevice, s));
   // This buffer's previous copy out of order_host must finish before it is rewritten.
   if (ctx->used) CKV(cudaEventSynchronize(ctx->ev[0]));
-  longest_first(b->d, b->n_docs, ctx->order_host);
+  const DocSplit split = split_longest_first(b->d, b->n_docs, ctx->order_host, g.K);
   CKV(cudaMemcpyAsync(ctx->order, ctx->order_host.data(), db, cudaMemcpyHostToDevice, s));
   CKV(cudaEventRecord(ctx->ev[0], s));
   if (z_step_async(s, (u32*)b->gpu_z, (const u32*)b->gpu_w, (const u32*)b->gpu_d_len, (u32*)b->gpu_d_idx,
-                   ctx->order, (u32*)b->gpu_K_d, b->n_docs, b->n_tokens, true, g.z_ev))
+                   ctx->order, (u32*)b->gpu_K_d, b->n_docs, b->n_tokens, true, g.z_ev, &split))
     return;
   g.z_timed = true;
   CKV(cudaMemcpyAsync(b->z, b->gpu_z, tb, cudaMemcpyDeviceToHost, s));
@@ -627,7 +682,7 @@ extern "C" int gpulda_corpus_load(const uint32_t* z, const uint32_t* w, const ui
   CK(cudaMemcpy(g.cw, w, n_tokens * 4, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(g.cd_len, d_len, (size_t)n_docs * 4, cudaMemcpyHostToDevice));
   std::vector<u32> order;
-  longest_first(d_len, n_docs, order);
+  g.c_split = split_longest_first(d_len, n_docs, order, g.K);
   CK(cudaMemcpy(g.corder, order.data(), (size_t)n_docs * 4, cudaMemcpyHostToDevice));
   launch_doc_offsets(g.cd_len, g.cd_idx, n_docs, g.stream);
   CK(cudaGetLastError());
@@ -643,7 +698,8 @@ extern "C" int gpulda_corpus_sweep(uint32_t n_iter) {
   for (u32 i = 0; i < n_iter; ++i) {
     int rc = phi_step_async(s);
     if (rc) return rc;
-    rc = z_step_async(s, g.cz, g.cw, g.cd_len, g.cd_idx, g.corder, g.cK_d, g.c_docs, g.c_tokens, false, g.z_ev);
+    rc = z_step_async(s, g.cz, g.cw, g.cd_len, g.cd_idx, g.corder, g.cK_d, g.c_docs, g.c_tokens, false, g.z_ev,
+                      &g.c_split);
     if (rc) return rc;
     g.z_timed = true;
   }

@@ -66,6 +66,11 @@ void launch_doc_offsets(const u32* d_len, u32* d_idx, u32 n_docs, cudaStream_t s
 // One sweep over a set of documents.
 void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s);
 size_t z_sweep_smem_per_warp(u32 K);
+// The same sweep with each document's counts in a shared-memory hash map
+// (large K).  Documents longer than lmax are reported, not swept.  Returns
+// false without launching when lmax needs more shared memory than a block has.
+bool launch_z_sweep_map(const ModelDev& m, const ZLaunch& z, cudaStream_t s, u32 lmax);
+u32 z_map_slots(u32 K, u32 lmax);
 
 // Debug hooks.
 void launch_debug_philox(const u32* ctr, u32 n, u32 k0, u32 k1, u32* out, cudaStream_t s);
