@@ -127,18 +127,17 @@ struct PoisTables {
 // Poisson(lambda) for lambda >= 10 by transformed rejection with squeeze
 // (W. Hoermann, "The transformed rejection method for generating Poisson
 // random variables", Insurance: Mathematics and Economics 12, 1993).
-// Attempt a uses Philox block (index, t, stream, a); attempt 0 reuses `r0`.
-static __device__ __noinline__ u32 poisson_ptrs(double lam, U4 r0, u64 index, u32 t, u32 stream,
-                                         u32 k0, u32 k1, const double* __restrict__ lfac) {
+// Attempt a uses Philox block (index, t, stream, 1 + a).
+static __device__ __noinline__ u32 poisson_ptrs(double lam, u64 index, u32 t, u32 stream, u32 k0, u32 k1,
+                                                const double* __restrict__ lfac) {
   const double slam = __dsqrt_rn(lam);
   const double loglam = det_log(lam);
   const double b = __dadd_rn(0.931, __dmul_rn(2.53, slam));
   const double a = __dadd_rn(-0.059, __dmul_rn(0.02483, b));
   const double inv_alpha = __dadd_rn(1.1239, __ddiv_rn(1.1328, __dadd_rn(b, -3.4)));
   const double vr = __dadd_rn(0.9277, -__ddiv_rn(3.6224, __dadd_rn(b, -2.0)));
-  U4 r = r0;
   for (u32 att = 0; att < kPtrsMaxAttempts; ++att) {
-    if (att > 0) r = draw4(index, t, stream, att, k0, k1);
+    const U4 r = draw4(index, t, stream, 1 + att, k0, k1);
     const double U = __dadd_rn(u53(r.x, r.y), -0.5);
     const double V = u53(r.z, r.w);
     const double us = __dadd_rn(0.5, -fabs(U));
@@ -153,23 +152,30 @@ static __device__ __noinline__ u32 poisson_ptrs(double lam, U4 r0, u64 index, u3
   return (u32)floor(lam);  // reached with probability far below 2^-100
 }
 
-// x ~ Poisson(n + beta).  n < kPoisN: inversion of the 32-bit CDF table with
-// word r.x; otherwise transformed rejection.
-__device__ __forceinline__ u32 poisson_draw(u32 n, double beta, U4 r, u64 index, u32 t, u32 stream,
+// Cells share Philox blocks: cell c's inversion word is word (c & 3) of the
+// block with counter index c >> 2 and sub-draw 0.
+__device__ __forceinline__ u32 u4_word(const U4& r, u32 i) {
+  return i == 0 ? r.x : i == 1 ? r.y : i == 2 ? r.z : r.w;
+}
+
+// x ~ Poisson(n + beta) for cell `index`.  n < kPoisN: inversion of the 32-bit
+// CDF table with the cell's word `ru`; otherwise transformed rejection.
+__device__ __forceinline__ u32 poisson_draw(u32 n, double beta, u32 ru, u64 index, u32 t, u32 stream,
                                             u32 k0, u32 k1, const PoisTables& tb) {
   if (n < kPoisN) {
     const u32* row = tb.cdf + (size_t)n * kPoisW;
-    u32 j = tb.guide[n * 256u + (r.x >> 24)];
-    while (j < kPoisW - 1 && r.x >= __ldg(row + j)) ++j;
+    u32 j = tb.guide[n * 256u + (ru >> 24)];
+    while (j < kPoisW - 1 && ru >= __ldg(row + j)) ++j;
     return j;
   }
-  return poisson_ptrs(__dadd_rn((double)n, beta), r, index, t, stream, k0, k1, tb.lfac);
+  return poisson_ptrs(__dadd_rn((double)n, beta), index, t, stream, k0, k1, tb.lfac);
 }
 
-// Alias entry: low word = threshold in units of 2^-32 of a slot, high word =
-// alias topic.  Slot s keeps its own topic when r < threshold.
-__device__ __forceinline__ u32 alias_pick(u64 entry, u32 slot, u32 r) {
-  return r < (u32)entry ? slot : (u32)(entry >> 32);
+// Alias entry of a word's sparse table (one slot per topic with q > 0):
+// bits 0-31 keep-threshold in units of 2^-32 of a slot, bits 32-47 the slot's
+// own topic, bits 48-63 its alias topic.  The slot keeps its topic when r < threshold.
+__device__ __forceinline__ u32 alias_pick(u64 entry, u32 r) {
+  return r < (u32)entry ? (u32)(entry >> 32) & 0xffffu : (u32)(entry >> 48);
 }
 
 // floor(r * B / 2^32) for r < 2^32, exact.

@@ -814,7 +814,7 @@ extern "C" int gpulda_debug_poisson(const uint32_t* count, const uint64_t* idx, 
 }
 
 extern "C" int gpulda_debug_alias(const uint32_t* q, uint32_t K, uint64_t* table_out) {
-  if (K < 1 || K > 12288) return fail(GPULDA_ERR_UNSUPPORTED, "debug_alias supports 1 <= K <= 12288");
+  if (K < 1 || K > 11264) return fail(GPULDA_ERR_UNSUPPORTED, "debug_alias supports 1 <= K <= 11264");
   u32* dq = nullptr;
   u64* dout = nullptr;
   int rc;

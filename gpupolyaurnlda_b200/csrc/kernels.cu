@@ -21,24 +21,32 @@ namespace {
 
 // ---------------------------------------------------------------------------
 // Initial counts (reference: polya_urn_init, src/cu/polyaurn.cu:61-79):
-// n[w][k] ~ Poisson(beta + floor(C[w] / K)).
+// n[w][k] ~ Poisson(beta + floor(C[w] / K)).  One Philox block serves the
+// four cells 4g .. 4g+3.
 // ---------------------------------------------------------------------------
 __global__ void init_counts_kernel(ModelDev m, const u32* __restrict__ C) {
   const u64 cells = (u64)m.K * m.V;
-  for (u64 c = (u64)blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += (u64)gridDim.x * blockDim.x) {
-    const u32 w = (u32)(c / m.K);
-    const u32 lam_n = C[w] / m.K;
-    const U4 r = draw4(c, 0, kStreamInitCounts, 0, m.key0, m.key1);
-    m.n[c] = poisson_draw(lam_n, (double)m.beta, r, c, 0, kStreamInitCounts, m.key0, m.key1, m.tables);
+  const u64 groups = (cells + 3) / 4;
+  for (u64 gi = (u64)blockIdx.x * blockDim.x + threadIdx.x; gi < groups; gi += (u64)gridDim.x * blockDim.x) {
+    const U4 r = draw4(gi, 0, kStreamInitCounts, 0, m.key0, m.key1);
+#pragma unroll
+    for (u32 u = 0; u < 4; ++u) {
+      const u64 c = gi * 4 + u;
+      if (c < cells) {
+        const u32 lam_n = C[c / m.K] / m.K;
+        m.n[c] = poisson_draw(lam_n, (double)m.beta, u4_word(r, u), c, 0, kStreamInitCounts, m.key0, m.key1,
+                              m.tables);
+      }
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Phi draw (reference: polya_urn_sample + draw_poisson + polya_urn_reset,
 // src/cu/polyaurn.cu:7-36,87-141).  Each block owns a contiguous range of
-// rows; threads stride over its cells (coalesced for any K).  Per-topic sums
-// are gathered in shared memory (integer atomics: order-free) and flushed once
-// per block.
+// rows; threads take groups of four cells (one Philox block, 16-byte loads and
+// stores when the group lies inside the range).  Per-topic sums are gathered
+// in shared memory (integer atomics: order-free) and flushed once per block.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) phi_draw_kernel(ModelDev m, u32 t, u32 rows_per_block, int smem_sums) {
   extern __shared__ unsigned long long s_sum[];
@@ -51,18 +59,46 @@ __global__ void __launch_bounds__(256) phi_draw_kernel(ModelDev m, u32 t, u32 ro
   const u32 w1 = min(m.V, w0 + rows_per_block);
   const u64 c0 = (u64)w0 * K, c1 = (u64)w1 * K;
   const double beta = (double)m.beta;
-  for (u64 c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-    const u32 nk = m.n[c];
-    const U4 r = draw4(c, t, kStreamPhi, 0, m.key0, m.key1);
-    const u32 x = poisson_draw(nk, beta, r, c, t, kStreamPhi, m.key0, m.key1, m.tables);
-    m.q[c] = x;
-    m.n[c] = 0;
-    if (x) {
-      const u32 k = (u32)(c % K);
-      if (smem_sums)
-        atomicAdd(&s_sum[k], (unsigned long long)x);
-      else
-        atomicAdd((unsigned long long*)&m.S[k], (unsigned long long)x);
+  for (u64 gi = c0 / 4 + threadIdx.x; gi * 4 < c1; gi += blockDim.x) {
+    const u64 cb = gi * 4;
+    const U4 r = draw4(gi, t, kStreamPhi, 0, m.key0, m.key1);
+    const bool whole = cb >= c0 && cb + 4 <= c1;
+    u32 nv[4];
+    if (whole) {
+      const uint4 v = *reinterpret_cast<const uint4*>(m.n + cb);
+      nv[0] = v.x;
+      nv[1] = v.y;
+      nv[2] = v.z;
+      nv[3] = v.w;
+    } else {
+#pragma unroll
+      for (u32 u = 0; u < 4; ++u) nv[u] = (cb + u >= c0 && cb + u < c1) ? m.n[cb + u] : 0u;
+    }
+    u32 xv[4];
+#pragma unroll
+    for (u32 u = 0; u < 4; ++u) {
+      const u64 c = cb + u;
+      xv[u] = poisson_draw(nv[u], beta, u4_word(r, u), c, t, kStreamPhi, m.key0, m.key1, m.tables);
+    }
+    if (whole) {
+      *reinterpret_cast<uint4*>(m.q + cb) = make_uint4(xv[0], xv[1], xv[2], xv[3]);
+      *reinterpret_cast<uint4*>(m.n + cb) = make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (u32 u = 0; u < 4; ++u) {
+      const u64 c = cb + u;
+      if (c < c0 || c >= c1) continue;
+      if (!whole) {
+        m.q[c] = xv[u];
+        m.n[c] = 0;
+      }
+      if (xv[u]) {
+        const u32 k = (u32)(c % K);
+        if (smem_sums)
+          atomicAdd(&s_sum[k], (unsigned long long)xv[u]);
+        else
+          atomicAdd((unsigned long long*)&m.S[k], (unsigned long long)xv[u]);
+      }
     }
   }
   if (smem_sums) {
@@ -73,10 +109,10 @@ __global__ void __launch_bounds__(256) phi_draw_kernel(ModelDev m, u32 t, u32 ro
 }
 
 // ---------------------------------------------------------------------------
-// Deterministic parallel alias construction over one row of integer weights
+// Deterministic parallel alias construction over n items with integer weights
 // (reference: build_alias, src/cu/spalias.cu:88-174, which uses atomic work
-// queues).  Slot capacity is A = sum_k q_k; item k carries w_k = K*q_k.
-// Items with w_k < A are light, the rest heavy, each list in ascending k.
+// queues).  Slot capacity is A = sum_i q_i; item i carries w_i = n*q_i.
+// Items with w_i < A are light, the rest heavy, each list in item order.
 // The result equals the sequential sweep in which the front heavy fills the
 // next light and, on falling below A, is itself filled by the following
 // heavy before any further light.  With D_i the exclusive prefix of light
@@ -86,23 +122,25 @@ __global__ void __launch_bounds__(256) phi_draw_kernel(ModelDev m, u32 t, u32 ro
 //               A - (D_i + d_i - E_j) with i the light whose deficit interval
 //               [D_i, D_i + d_i) contains E_j;
 //   other heavies keep the whole slot.
-// Every quantity is an exact integer (K <= 32768 keeps K*A below 2^63).
-// sq[K] holds q; vals[K] and idx[K] are scratch.  Block-cooperative.
+// Every quantity is an exact integer (n <= K <= 32768 keeps n*A below 2^63).
+// Entry of item i: threshold | key[i] << 32 | key[alias item] << 48.
+// wq[n] holds the weights, key[n] the items' topics; vals[n], idx[n] scratch.
+// Block-cooperative.
 // ---------------------------------------------------------------------------
-__device__ void alias_build_block(const u64* sq, u32 K, u64 A, u64* vals, uint16_t* idx,
-                                  u64* out_row, u64* sh) {
+__device__ void alias_build_block(const u64* wq, const uint16_t* key, u32 n, u64 A, u64* vals, uint16_t* idx,
+                                  u64* out, u64* sh) {
   const u32 NT = blockDim.x, tid = threadIdx.x;
-  const u32 chunk = (K + NT - 1) / NT;
-  const u32 k0 = min(K, tid * chunk), k1 = min(K, k0 + chunk);
+  const u32 chunk = (n + NT - 1) / NT;
+  const u32 i0 = min(n, tid * chunk), i1 = min(n, i0 + chunk);
   u64 nl = 0, dl = 0, nh = 0, eh = 0;
-  for (u32 k = k0; k < k1; ++k) {
-    const u64 wk = (u64)K * sq[k];
-    if (wk < A) {
+  for (u32 i = i0; i < i1; ++i) {
+    const u64 wi = (u64)n * wq[i];
+    if (wi < A) {
       ++nl;
-      dl += A - wk;
+      dl += A - wi;
     } else {
       ++nh;
-      eh += wk - A;
+      eh += wi - A;
     }
   }
   u64 nL, Dtot, nH, Etot;
@@ -110,17 +148,17 @@ __device__ void alias_build_block(const u64* sq, u32 K, u64 A, u64* vals, uint16
   u64 od = block_excl_scan_u64(dl, sh, &Dtot);
   u64 oh = block_excl_scan_u64(nh, sh, &nH);
   u64 oe = block_excl_scan_u64(eh, sh, &Etot);
-  for (u32 k = k0; k < k1; ++k) {
-    const u64 wk = (u64)K * sq[k];
-    if (wk < A) {
+  for (u32 i = i0; i < i1; ++i) {
+    const u64 wi = (u64)n * wq[i];
+    if (wi < A) {
       vals[ol] = od;
-      idx[ol] = (uint16_t)k;
-      od += A - wk;
+      idx[ol] = (uint16_t)i;
+      od += A - wi;
       ++ol;
     } else {
-      oe += wk - A;
+      oe += wi - A;
       vals[nL + oh] = oe;
-      idx[nL + oh] = (uint16_t)k;
+      idx[nL + oh] = (uint16_t)i;
       ++oh;
     }
   }
@@ -135,7 +173,7 @@ __device__ void alias_build_block(const u64* sq, u32 K, u64 A, u64* vals, uint16
       if (Ev[mid] >= D) hi = mid; else lo = mid + 1;
     }
     const u32 l = idx[i];
-    out_row[l] = ((u64)Hi[lo] << 32) | alias_threshold((u64)K * sq[l], A);
+    out[l] = ((u64)key[Hi[lo]] << 48) | ((u64)key[l] << 32) | alias_threshold((u64)n * wq[l], A);
   }
   for (u32 j = tid; j < (u32)nH; j += NT) {
     const u32 h = Hi[j];
@@ -146,16 +184,18 @@ __device__ void alias_build_block(const u64* sq, u32 K, u64 A, u64* vals, uint16
         const u32 mid = (lo + hi + 1) >> 1;
         if (vals[mid] <= E) lo = mid; else hi = mid - 1;
       }
-      const u64 d = A - (u64)K * sq[idx[lo]];
+      const u64 d = A - (u64)n * wq[idx[lo]];
       const u64 over = vals[lo] + d - E;
-      out_row[h] = ((u64)Hi[j + 1] << 32) | alias_threshold(A - over, A);
+      out[h] = ((u64)key[Hi[j + 1]] << 48) | ((u64)key[h] << 32) | alias_threshold(A - over, A);
     } else {
-      out_row[h] = ((u64)h << 32) | 0xffffffffu;
+      out[h] = ((u64)key[h] << 48) | ((u64)key[h] << 32) | 0xffffffffu;
     }
   }
 }
 
-// Per word: q = floor(x * 2^32 / S[k]) (clamped), A, nnz, alias table.
+// Per word: q = floor(x * 2^32 / S[k]) (clamped) written back densely; the
+// word's topics with q > 0 compacted in ascending order (nnz, the per-word
+// list q << 32 | k, the dense mass A) and the sparse alias table over them.
 // Persistent blocks loop over words; scratch is shared memory or, for large
 // K, a per-block slice of global memory.
 __global__ void __launch_bounds__(256) alias_build_kernel(ModelDev m, unsigned char* gscratch, size_t slice) {
@@ -163,41 +203,40 @@ __global__ void __launch_bounds__(256) alias_build_kernel(ModelDev m, unsigned c
   __shared__ u64 sh[33];
   const u32 K = m.K;
   unsigned char* base = gscratch ? gscratch + (size_t)blockIdx.x * slice : s_raw;
-  u64* sq = (u64*)base;
-  u64* vals = sq + K;
-  uint16_t* idx = (uint16_t*)(vals + K);
+  u64* cq = (u64*)base;        // compacted weights
+  u64* vals = cq + K;
+  uint16_t* ck = (uint16_t*)(vals + K);  // compacted topics
+  uint16_t* idx = ck + K;
   for (u32 w = blockIdx.x; w < m.V; w += gridDim.x) {
     const size_t row = (size_t)w * K;
-    u64 part = 0, cnt = 0;
-    for (u32 k = threadIdx.x; k < K; k += blockDim.x) {
-      const u32 x = m.q[row + k];
+    u64 part = 0, nz = 0;
+    for (u32 t0 = 0; t0 < K; t0 += blockDim.x) {
+      const u32 k = t0 + threadIdx.x;
       u64 qq = 0;
-      if (x) {
-        qq = (((u64)x) << 32) / m.S[k];
-        if (qq > 0xffffffffULL) qq = 0xffffffffULL;
-        ++cnt;
+      if (k < K) {
+        const u32 x = m.q[row + k];
+        if (x) {
+          qq = (((u64)x) << 32) / m.S[k];
+          if (qq > 0xffffffffULL) qq = 0xffffffffULL;
+        }
+        m.q[row + k] = (u32)qq;
       }
-      m.q[row + k] = (u32)qq;
-      sq[k] = qq;
+      u64 tile;
+      const u64 pos = nz + block_excl_scan_u64(qq != 0, sh, &tile);
+      if (qq) {
+        cq[pos] = qq;
+        ck[pos] = (uint16_t)k;
+      }
+      nz += tile;
       part += qq;
     }
-    const u64 A = block_sum_u64(part, sh);
-    const u64 nz = block_sum_u64(cnt, sh);
-    alias_build_block(sq, K, A, vals, idx, m.al + row, sh);
-    {
-      // the word's nonzero q in ascending k (thread chunks are contiguous)
-      const u32 chunk = (K + blockDim.x - 1) / blockDim.x;
-      const u32 k0 = min(K, threadIdx.x * chunk), k1 = min(K, k0 + chunk);
-      u64 c = 0;
-      for (u32 k = k0; k < k1; ++k) c += sq[k] != 0;
-      u64 tot;
-      u64 pos = block_excl_scan_u64(c, sh, &tot);
-      for (u32 k = k0; k < k1; ++k)
-        if (sq[k]) m.csr[row + pos++] = (sq[k] << 32) | k;
-    }
+    const u64 A = block_sum_u64(part, sh);  // (also a barrier for cq/ck)
+    const u32 n = (u32)nz;
+    for (u32 i = threadIdx.x; i < n; i += blockDim.x) m.csr[row + i] = (cq[i] << 32) | ck[i];
+    if (n) alias_build_block(cq, ck, n, A, vals, idx, m.al + row, sh);
     if (threadIdx.x == 0) {
       m.A[w] = A;
-      m.nnz[w] = (u32)nz;
+      m.nnz[w] = n;
     }
     __syncthreads();
   }
@@ -208,14 +247,16 @@ __global__ void debug_alias_kernel(const u32* q, u32 K, u64* out) {
   __shared__ u64 sh[33];
   u64* sq = (u64*)s_raw;
   u64* vals = sq + K;
-  uint16_t* idx = (uint16_t*)(vals + K);
+  uint16_t* key = (uint16_t*)(vals + K);
+  uint16_t* idx = key + K;
   u64 part = 0;
   for (u32 k = threadIdx.x; k < K; k += blockDim.x) {
     sq[k] = q[k];
+    key[k] = (uint16_t)k;
     part += q[k];
   }
   const u64 A = block_sum_u64(part, sh);
-  alias_build_block(sq, K, A, vals, idx, out, sh);
+  alias_build_block(sq, key, K, A, vals, idx, out, sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -251,8 +292,9 @@ __global__ void debug_poisson_kernel(ModelDev m, const u32* count, const u64* id
                                      u32 k0, u32 k1, u32* out) {
   const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const U4 r = draw4(idx[i], t, stream, 0, k0, k1);
-  out[i] = poisson_draw(count[i], (double)m.beta, r, idx[i], t, stream, k0, k1, m.tables);
+  const U4 r = draw4(idx[i] >> 2, t, stream, 0, k0, k1);
+  out[i] = poisson_draw(count[i], (double)m.beta, u4_word(r, (u32)(idx[i] & 3)), idx[i], t, stream, k0, k1,
+                        m.tables);
 }
 
 }  // namespace
@@ -290,7 +332,7 @@ static u32 alias_threads(u32 K) {
   return 32 * nw;
 }
 
-static size_t alias_smem_bytes(u32 K) { return ((size_t)K * 18 + 15) & ~(size_t)15; }
+static size_t alias_smem_bytes(u32 K) { return ((size_t)K * 20 + 15) & ~(size_t)15; }
 
 constexpr size_t kMaxDynSmem = 200 * 1024;
 

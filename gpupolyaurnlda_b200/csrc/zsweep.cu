@@ -182,10 +182,11 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
       // Per-token word data for the whole chunk, loaded lane-parallel so the
       // token loop never waits on them: nnz, dense mass, and the alias entry
       // of the slot this token's dense draw would use.
-      const u32 my_s = (u32)(((u64)r.z * K) >> 32);
+      // the dense draw's slot in the word's sparse alias table (nnz slots)
       const u32 my_nw = valid ? __ldg(m.nnz + my_w) : 0u;
       const u64 my_A = valid ? __ldg(m.A + my_w) : 0ull;
-      const u64 my_al = valid ? __ldg(m.al + (size_t)my_w * K + my_s) : 0ull;
+      const u32 my_s = (u32)(((u64)r.z * my_nw) >> 32);
+      const u64 my_al = (valid && my_nw) ? __ldg(m.al + (size_t)my_w * K + my_s) : 0ull;
       u32 new_z = my_z;
       const u32 nt = min(32u, L - base);
       for (u32 j = 0; j < nt; ++j) {
@@ -258,9 +259,8 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
             }
           } else {
             const u32 r3 = __shfl_sync(kFullMask, r.w, j);
-            const u32 s = __shfl_sync(kFullMask, my_s, j);
             const u64 e = __shfl_sync(kFullMask, my_al, j);
-            k = alias_pick(e, s, r3);
+            k = alias_pick(e, r3);
           }
         }
         // add the new topic

@@ -199,10 +199,11 @@ __global__ void __launch_bounds__(256, 4) z_sweep_map_kernel(MapArgs a) {
       }
       if (my_z >= K) my_z %= K;
       const U4 r = draw4(p.tok_base + off + i, p.t, kStreamZ, 0, m.key0, m.key1);
-      const u32 my_s = (u32)(((u64)r.z * K) >> 32);
+      // the dense draw's slot in the word's sparse alias table (nnz slots)
       const u32 my_nw = valid ? __ldg(m.nnz + my_w) : 0u;
       const u64 my_A = valid ? __ldg(m.A + my_w) : 0ull;
-      const u64 my_al = valid ? __ldg(m.al + (size_t)my_w * K + my_s) : 0ull;
+      const u32 my_s = (u32)(((u64)r.z * my_nw) >> 32);
+      const u64 my_al = (valid && my_nw) ? __ldg(m.al + (size_t)my_w * K + my_s) : 0ull;
       u32 new_z = my_z;
       const u32 nt = min(32u, L - base);
       for (u32 j = 0; j < nt; ++j) {
@@ -252,9 +253,8 @@ __global__ void __launch_bounds__(256, 4) z_sweep_map_kernel(MapArgs a) {
             }
           } else {
             const u32 r3 = __shfl_sync(kFullMask, r.w, j);
-            const u32 s = __shfl_sync(kFullMask, my_s, j);
             const u64 e = __shfl_sync(kFullMask, my_al, j);
-            k = alias_pick(e, s, r3);
+            k = alias_pick(e, r3);
           }
         }
         const u32 nw = __shfl_sync(kFullMask, my_nw, j);

@@ -47,6 +47,7 @@ def lib() -> C.CDLL:
         L.orc_phi_step.argtypes = [C.c_uint32, C.c_uint32, C.c_float, _U32P, C.c_uint32, C.c_uint32, C.c_uint32,
                                    _U32P, _U64P, _U64P, _U64P, _U32P, C.c_int]
         L.orc_alias.argtypes = [_U32P, C.c_uint32, _U64P]
+        L.orc_alias_items.argtypes = [_U32P, C.POINTER(C.c_uint16), C.c_uint32, _U64P]
         L.orc_doc_offsets.argtypes = [_U32P, C.c_uint32, _U64P]
         L.orc_z_sweep.argtypes = [C.c_uint32, C.c_uint32, C.c_float, _U32P, _U64P, _U64P, _U32P, _U32P, _U32P,
                                   _U32P, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, _U32P, _U64P,
@@ -127,6 +128,22 @@ def alias(q: np.ndarray) -> np.ndarray:
     out = np.empty(len(q), np.uint64)
     lib().orc_alias(_p32(q), len(q), _p64(out))
     return out
+
+
+def alias_items(q: np.ndarray, keys: np.ndarray) -> np.ndarray:
+    """Alias table over len(q) items whose topics are `keys`."""
+    q = np.ascontiguousarray(q, np.uint32)
+    keys = np.ascontiguousarray(keys, np.uint16)
+    out = np.empty(len(q), np.uint64)
+    lib().orc_alias_items(_p32(q), keys.ctypes.data_as(C.POINTER(C.c_uint16)), len(q), _p64(out))
+    return out
+
+
+def live_alias_entries(alias: np.ndarray, nnz: np.ndarray, K: int) -> np.ndarray:
+    """The entries a model uses: the first nnz[w] of each word's row."""
+    V = len(nnz)
+    mask = np.arange(K)[None, :] < nnz.astype(np.int64)[:, None]
+    return alias.reshape(V, K)[mask]
 
 
 def alias_draw(table: np.ndarray, r_slot: int, r_keep: int) -> int:

@@ -140,8 +140,9 @@ double log_fact(i64 k, const Tables& T) {
   return r + corr;
 }
 
-// Hoermann (1993) transformed rejection for lambda >= 10.
-u32 ptrs(double lam, W4 r, u64 idx, u32 t, u32 stream, u32 k0, u32 k1, const Tables& T) {
+// Hoermann (1993) transformed rejection for lambda >= 10; attempt a draws the
+// Philox block (idx, t, stream, sub 1 + a).
+u32 ptrs(double lam, u64 idx, u32 t, u32 stream, u32 k0, u32 k1, const Tables& T) {
   const double slam = std::sqrt(lam);
   const double loglam = det_log(lam);
   const double b = 0.931 + 2.53 * slam;
@@ -149,7 +150,7 @@ u32 ptrs(double lam, W4 r, u64 idx, u32 t, u32 stream, u32 k0, u32 k1, const Tab
   const double inv_alpha = 1.1239 + 1.1328 / (b + -3.4);
   const double vr = 0.9277 + -(3.6224 / (b + -2.0));
   for (u32 att = 0; att < PTRS_MAX; ++att) {
-    if (att > 0) r = draw(idx, t, stream, att, k0, k1);
+    const W4 r = draw(idx, t, stream, 1 + att, k0, k1);
     const double U = unit53(r.v[0], r.v[1]) + -0.5;
     const double V = unit53(r.v[2], r.v[3]);
     const double us = 0.5 + -std::fabs(U);
@@ -164,14 +165,21 @@ u32 ptrs(double lam, W4 r, u64 idx, u32 t, u32 stream, u32 k0, u32 k1, const Tab
   return (u32)std::floor(lam);
 }
 
-u32 poisson(u32 n, float beta, W4 r, u64 idx, u32 t, u32 stream, u32 k0, u32 k1, const Tables& T) {
+// Cell idx's inversion word: word (idx & 3) of the Philox block (idx >> 2, t,
+// stream, sub 0) -- four cells share one block.
+u32 cell_word(u64 idx, u32 t, u32 stream, u32 k0, u32 k1) {
+  return draw(idx >> 2, t, stream, 0, k0, k1).v[idx & 3];
+}
+
+u32 poisson(u32 n, float beta, u64 idx, u32 t, u32 stream, u32 k0, u32 k1, const Tables& T) {
   if (n < POIS_N) {
+    const u32 u = cell_word(idx, t, stream, k0, k1);
     const u32* row = &T.cdf[(size_t)n * POIS_W];
     u32 j = 0;  // plain linear inversion (the guide is only a shortcut)
-    while (j < POIS_W - 1 && r.v[0] >= row[j]) ++j;
+    while (j < POIS_W - 1 && u >= row[j]) ++j;
     return j;
   }
-  return ptrs((double)n + (double)beta, r, idx, t, stream, k0, k1, T);
+  return ptrs((double)n + (double)beta, idx, t, stream, k0, k1, T);
 }
 
 Tables& tables_for(float beta) {
@@ -186,9 +194,10 @@ u32 threshold(u64 p, u64 A) {
   return t >= 4294967295.0 ? 0xffffffffu : (u32)t;
 }
 
-// Sequential alias sweep over integer weights q (Vose's method with the heavy
-// that falls below the slot capacity filled next).
-void alias_seq(const u64* q, u32 K, u64* out) {
+// Sequential alias sweep over n items with integer weights q (Vose's method
+// with the heavy that falls below the slot capacity filled next).  Entry of
+// item i: threshold | key[i] << 32 | key[alias item] << 48.
+void alias_seq(const u64* q, const uint16_t* key, u32 K, u64* out) {
   u64 A = 0;
   for (u32 k = 0; k < K; ++k) A += q[k];
   std::vector<u64> w(K);
@@ -197,6 +206,9 @@ void alias_seq(const u64* q, u32 K, u64* out) {
     w[k] = (u64)K * q[k];
     (w[k] < A ? L : H).push_back(k);
   }
+  auto entry = [&](u32 item, u32 alias_item, u32 thr) {
+    return ((u64)key[alias_item] << 48) | ((u64)key[item] << 32) | thr;
+  };
   size_t li = 0, hj = 0;
   long pending = -1;
   while (true) {
@@ -210,18 +222,18 @@ void alias_seq(const u64* q, u32 K, u64* out) {
       break;
     }
     if (hj >= H.size()) {  // unreachable with exact integer weights
-      out[l] = ((u64)l << 32) | 0xffffffffu;
+      out[l] = entry(l, l, 0xffffffffu);
       continue;
     }
     const u32 h = H[hj];
-    out[l] = ((u64)h << 32) | threshold(w[l], A);
+    out[l] = entry(l, h, threshold(w[l], A));
     w[h] -= A - w[l];
     if (w[h] < A) {
       pending = h;
       ++hj;
     }
   }
-  for (; hj < H.size(); ++hj) out[H[hj]] = ((u64)H[hj] << 32) | 0xffffffffu;
+  for (; hj < H.size(); ++hj) out[H[hj]] = entry(H[hj], H[hj], 0xffffffffu);
 }
 
 template <class F>
@@ -243,6 +255,7 @@ void parallel_for(u64 n, int threads, F f) {
 }  // namespace
 
 extern "C" {
+u32 orc_alias_draw(const u64* table, u32 n, u32 r_slot, u32 r_keep);
 
 void orc_philox(const u32* ctr, u32 n, u32 k0, u32 k1, u32* out) {
   for (u32 i = 0; i < n; ++i) {
@@ -261,7 +274,7 @@ void orc_tables(float beta, u32* cdf, uint8_t* guide, double* lfac) {
 
 void orc_poisson(const u32* count, const u64* idx, u32 n, float beta, u32 t, u32 stream, u32 k0, u32 k1, u32* out) {
   const Tables& T = tables_for(beta);
-  for (u32 i = 0; i < n; ++i) out[i] = poisson(count[i], beta, draw(idx[i], t, stream, 0, k0, k1), idx[i], t, stream, k0, k1, T);
+  for (u32 i = 0; i < n; ++i) out[i] = poisson(count[i], beta, idx[i], t, stream, k0, k1, T);
 }
 
 double orc_log(double x) { return det_log(x); }
@@ -273,7 +286,7 @@ void orc_init_counts(u32 K, u32 V, float beta, const u32* C, u32 k0, u32 k1, u32
     for (u64 w = a; w < b; ++w)
       for (u32 k = 0; k < K; ++k) {
         const u64 c = w * K + k;
-        n[c] = poisson(C[w] / K, beta, draw(c, 0, STREAM_INIT, 0, k0, k1), c, 0, STREAM_INIT, k0, k1, T);
+        n[c] = poisson(C[w] / K, beta, c, 0, STREAM_INIT, k0, k1, T);
       }
   });
 }
@@ -291,7 +304,7 @@ void orc_phi_step(u32 K, u32 V, float beta, const u32* n, u32 t, u32 k0, u32 k1,
     for (u64 w = a; w < b; ++w)
       for (u32 k = 0; k < K; ++k) {
         const u64 c = w * K + k;
-        const u32 x = poisson(n[c], beta, draw(c, t, STREAM_PHI, 0, k0, k1), c, t, STREAM_PHI, k0, k1, T);
+        const u32 x = poisson(n[c], beta, c, t, STREAM_PHI, k0, k1, T);
         q[c] = x;
         ps[k] += x;
       }
@@ -301,11 +314,15 @@ void orc_phi_step(u32 K, u32 V, float beta, const u32* n, u32 t, u32 k0, u32 k1,
     for (int i = 0; i < nt; ++i) s += part[i][k];
     S[k] = s;
   }
+  // per word: the topics with q > 0 in ascending order carry the word's
+  // sparse alias table (entries 0 .. nnz-1 of the row; the rest unused)
   parallel_for(V, nt, [&](u64 a, u64 b, int) {
-    std::vector<u64> row(K);
+    std::vector<u64> row;
+    std::vector<uint16_t> keys;
     for (u64 w = a; w < b; ++w) {
       u64 sum = 0;
-      u32 nz = 0;
+      row.clear();
+      keys.clear();
       for (u32 k = 0; k < K; ++k) {
         const u64 c = w * K + k;
         const u32 x = q[c];
@@ -313,30 +330,43 @@ void orc_phi_step(u32 K, u32 V, float beta, const u32* n, u32 t, u32 k0, u32 k1,
         if (x) {
           v = ((u64)x << 32) / S[k];
           if (v > 0xffffffffULL) v = 0xffffffffULL;
-          ++nz;
         }
         q[c] = (u32)v;
-        row[k] = v;
+        if (v) {
+          row.push_back(v);
+          keys.push_back((uint16_t)k);
+        }
         sum += v;
       }
       A[w] = sum;
-      nnz[w] = nz;
-      alias_seq(row.data(), K, al + w * K);
+      nnz[w] = (u32)row.size();
+      std::fill(al + w * K, al + w * K + K, 0ull);
+      if (!row.empty()) alias_seq(row.data(), keys.data(), (u32)row.size(), al + w * K);
     }
   });
 }
 
+// Alias table over K items with topics 0..K-1.
 void orc_alias(const u32* q, u32 K, u64* out) {
   std::vector<u64> row(q, q + K);
-  alias_seq(row.data(), K, out);
+  std::vector<uint16_t> keys(K);
+  for (u32 k = 0; k < K; ++k) keys[k] = (uint16_t)k;
+  alias_seq(row.data(), keys.data(), K, out);
 }
 
-// Dense draw (reference draw_alias, src/cu/topics.cuh:63-83): slot =
-// floor(r_slot * K / 2^32); keep the slot when r_keep < threshold.
-u32 orc_alias_draw(const u64* table, u32 K, u32 r_slot, u32 r_keep) {
-  const u32 slot = (u32)(((u64)r_slot * K) >> 32);
+// Alias table over n items with the given topics.
+void orc_alias_items(const u32* q, const uint16_t* keys, u32 n, u64* out) {
+  std::vector<u64> row(q, q + n);
+  alias_seq(row.data(), keys, n, out);
+}
+
+// Dense draw (reference draw_alias, src/cu/topics.cuh:63-83) from a table of
+// n slots: slot = floor(r_slot * n / 2^32); the slot's own topic when
+// r_keep < threshold, else its alias topic.
+u32 orc_alias_draw(const u64* table, u32 n, u32 r_slot, u32 r_keep) {
+  const u32 slot = (u32)(((u64)r_slot * n) >> 32);
   const u64 e = table[slot];
-  return r_keep < (u32)e ? slot : (u32)(e >> 32);
+  return r_keep < (u32)e ? (u32)(e >> 32) & 0xffffu : (u32)(e >> 48);
 }
 
 // Sparse inverse CDF (reference draw_wary_search over the prefix of
@@ -446,9 +476,8 @@ void orc_z_sweep(u32 K, u32 V, float alpha, const u32* q, const u64* al, const u
               }
             }
         } else {
-          const u32 slot = (u32)(((u64)r.v[2] * K) >> 32);
-          const u64 e = al[row + slot];
-          k = r.v[3] < (u32)e ? slot : (u32)(e >> 32);
+          // dense part: the word's sparse alias table has nnz[wi] slots
+          k = orc_alias_draw(al + row, nnz[wi], r.v[2], r.v[3]);
         }
         s_S += std::min<u64>(nzd, nnz[wi]);
         s_sp += sparse ? 1 : 0;

@@ -85,6 +85,10 @@ def test_init_counts_match_oracle(gpu_lib, oracle_lib):
 
 
 def _compare_phi(st, phi):
+    import oracle
+    K = len(st["S"])
+    st = dict(st, alias=oracle.live_alias_entries(st["alias"], st["nnz"], K))
+    phi = dict(phi, alias=oracle.live_alias_entries(phi["alias"], phi["nnz"], K))
     for key in ("S", "q", "A", "nnz", "alias"):
         a, b = st[key], phi[key]
         if not (a == b).all():

@@ -48,14 +48,17 @@ def test_det_log_accuracy(oracle_lib):
 
 
 # --- src/cu/test/test_spalias.cu:14-53 ---------------------------------------
-def _alias_distribution(table: np.ndarray) -> np.ndarray:
-    K = len(table)
+def _alias_distribution(table: np.ndarray, K: int | None = None) -> np.ndarray:
+    """Topic distribution of a table (entry: threshold | own << 32 | alias << 48)."""
+    n = len(table)
+    K = K or n
     thr = (table & 0xffffffff).astype(np.float64)
-    ali = (table >> 32).astype(np.int64)
+    own = ((table >> 32) & 0xffff).astype(np.int64)
+    ali = (table >> 48).astype(np.int64)
     keep = np.where(thr == 0xffffffff, 1.0, thr / TWO32)
     p = np.zeros(K)
-    np.add.at(p, np.arange(K), keep / K)
-    np.add.at(p, ali, (1 - keep) / K)
+    np.add.at(p, own, keep / n)
+    np.add.at(p, ali, (1 - keep) / n)
     return p
 
 
@@ -64,7 +67,8 @@ def test_alias_reference_vector(oracle_lib):
     # everyone's alias and keeps its own slot.
     q = np.array([90, 2] + [1] * 8, np.uint32)
     t = oracle_lib.alias(q)
-    assert ((t >> 32) == 0).all()
+    assert ((t >> 48) == 0).all()
+    assert (((t >> 32) & 0xffff) == np.arange(10)).all()
     keep = (t & 0xffffffff)
     assert keep[0] == 0xffffffff
     assert keep[1] == int(0.2 * TWO32) and (keep[2:] == int(0.1 * TWO32)).all()
@@ -82,9 +86,13 @@ def test_alias_distribution_random(oracle_lib):
             p = _alias_distribution(t)
             assert np.allclose(p, q / q.astype(np.float64).sum(), atol=K * 2.0 ** -31)
             # zero-weight topics are never returned
-            ali = (t >> 32).astype(np.int64)
+            ali = (t >> 48).astype(np.int64)
             keep = t & 0xffffffff
             assert (q[ali[keep != 0xffffffff]] > 0).all()
+            # the sparse form over the nonzero items gives the same distribution
+            nzk = np.nonzero(q)[0]
+            ts = oracle_lib.alias_items(q[nzk], nzk.astype(np.uint16))
+            assert np.allclose(_alias_distribution(ts, K), q / q.astype(np.float64).sum(), atol=K * 2.0 ** -31)
 
 
 # --- src/cu/test/test_topics.cu:16-47 ----------------------------------------
@@ -99,7 +107,7 @@ def test_doc_offsets_reference_vector(oracle_lib):
 # --- src/cu/test/test_topics.cu:49-76 ----------------------------------------
 def test_alias_draw_reference_vector(oracle_lib):
     K = 5
-    table = np.array([(1 << 32) | (TWO32 // 2)] * K, np.uint64)
+    table = np.array([(1 << 48) | (s << 32) | (TWO32 // 2) for s in range(K)], np.uint64)
     # The reference draws with u = 0.6f (slot 3, remainder ~0 < .5 -> 3) and
     # u = 0.75f (slot 3, remainder .75 >= .5 -> alias 1); the slot word here is
     # u * 2^32 and the keep word is the remainder * 2^32.
@@ -193,7 +201,10 @@ def test_phi_step_matches_direct_computation(oracle_lib):
     assert (phi["q"] == q).all()
     assert (phi["nnz"] == (x.reshape(V, K) > 0).sum(1)).all()
     for w in range(V):
-        assert (phi["alias"][w * K:(w + 1) * K] == oracle_lib.alias(phi["q"][w * K:(w + 1) * K])).all()
+        row = phi["q"][w * K:(w + 1) * K]
+        nzk = np.nonzero(row)[0]
+        assert phi["nnz"][w] == len(nzk)
+        assert (phi["alias"][w * K:w * K + len(nzk)] == oracle_lib.alias_items(row[nzk], nzk.astype(np.uint16))).all()
 
 
 # --- src/cu/test/test_topics.cu:276-334 --------------------------------------
