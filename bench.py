@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU seconds per timed oracle iteration")
+    p.add_argument("--problems", type=int, default=64, help="batched workload: number of problems")
+    p.add_argument("--batch-scale", type=float, default=1.0, help="batched workload: scale of each problem's D")
+    p.add_argument("--tune-cache", default=None, help="batched workload: autotuner cache file")
     return p.parse_args()
 
 
@@ -251,7 +254,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     c = make_corpus(args, f"cuda:{local}")
     torch.cuda.synchronize()
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # the library's work and the timing events share it
     hbm, peak_kind = peaks()
 
     # ---- device-resident corpus: value + roofline ----------------------------
@@ -342,10 +345,123 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def batched_problems(args, device, chain: int):
+    """The batched-chains workload (corpus.batched_workloads): problem i drawn
+    with data seed 1000 + i, sampled with seed i and the given chain."""
+    from gpupolyaurnlda_b200 import corpus
+    from gpupolyaurnlda_b200.batch import ProblemSpec
+    specs = []
+    for i, wl in enumerate(corpus.batched_workloads(args.problems, seed=1, D_scale=args.batch_scale)):
+        c = corpus.generate(wl, seed=1000 + i, device=device)
+        specs.append(ProblemSpec(c.alpha, c.beta, c.K, c.counts, c.z, c.w, c.d_len, seed=i, chain=chain))
+    return specs
+
+
+def run_batched(args):
+    """Batched chains: all problems in one graph-replayed iteration, against
+    the same problems run one after another as solo models (the same
+    iterations, seeds and chains, so the final log-likelihoods must agree)."""
+    import torch
+    import torch.distributed as dist
+
+    import gpupolyaurnlda_b200 as g
+    from gpupolyaurnlda_b200.batch import BatchChains
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    t0 = time.perf_counter()
+    specs = batched_problems(args, f"cuda:{local}", rank)
+    t_gen = time.perf_counter() - t0
+    N = sum(len(sp.z) for sp in specs)
+    D = sum(len(sp.d_len) for sp in specs)
+    stream = torch.cuda.Stream()  # graph launches and timing events share it
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    t0 = time.perf_counter()
+    b = BatchChains(specs)
+    t_create = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    n_tuned = b.tune(args.tune_cache)
+    t_tune = time.perf_counter() - t0
+    shapes = b.shapes()
+    info = b.info()
+    b.sweep_async(args.warmup, stream.cuda_stream)
+    b.sync()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    b.sweep_async(args.steps, stream.cuda_stream)
+    e1.record(stream)
+    b.sync()
+    clk = clocks.stop()
+    ms_max = max_over_ranks(e0.elapsed_time(e1), f"cuda:{local}")
+    ll_b, _ = b.loglik()
+    b.close()
+
+    # the same problems one after another, each a solo model
+    seq_ms, ll_s = 0.0, []
+    for sp in specs:
+        s = g.Sampler(sp.alpha, sp.beta, sp.K, sp.counts, buffer_size=16, max_D=4, seed=sp.seed, chain=sp.chain,
+                      flags=g.GPULDA_FLAG_LOGLIK)
+        s.set_stream(stream.cuda_stream)
+        s.corpus_load(sp.z.copy(), sp.w, sp.d_len)
+        s.corpus_sweep(args.warmup)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.corpus_sweep(1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        seq_ms += e0.elapsed_time(e1)
+        ll_s.append(s.loglik()[0])
+        s.set_stream(0)
+        s.close()
+    seq_max = max_over_ranks(seq_ms, f"cuda:{local}")
+    rel = max(abs(a - c) / abs(c) for a, c in zip(ll_b, ll_s))
+    value = replica_value(N, args.steps, world, ms_max / 1e3)
+    seq_value = replica_value(N, args.steps, world, seq_max / 1e3)
+    if rank == 0:
+        Ks = [sp.K for sp in specs]
+        line = {"metric": "batched_gibbs_tokens_per_sec", "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                "data": "synthetic",
+                "config": {"workload": f"batched: {len(specs)} independent problems, K in {{50,200,1000}} "
+                                       f"({Ks.count(50)}/{Ks.count(200)}/{Ks.count(1000)}), V in [5k,50k], "
+                                       f"D in [1k,100k] x{args.batch_scale}, doc lengths lognormal(4.5,1.0); "
+                                       f"N={N} tokens, D={D} documents",
+                           "N": N, "D": D, "cells": info["cells"], "device_bytes": info["device_bytes"],
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                           "l2": "inputs larger than L2"},
+                "sequential": {"value": seq_value, "unit": UNIT, "ms_per_step": seq_max / args.steps,
+                               "what": "the same problems one after another as solo models (gpulda_corpus_sweep), "
+                                       "device time summed"},
+                "speedup_vs_sequential": value / seq_value,
+                "loglik_max_rel_diff_vs_solo": rel,
+                "autotuner": {"buckets_tuned": n_tuned, "seconds": t_tune,
+                              "shapes": {b_: list(sh) for b_, sh in zip(("K<=64", "K<=256", "K<=1024", "K<=2048"),
+                                                                         shapes) if sh[0]}},
+                "setup_seconds": {"generate": t_gen, "create": t_create},
+                "gpu_launches": args.steps * (1 + 3 * info["buckets"]), "clocks": clk}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched":
+        run_batched(args)
     else:
         run_ours(args)
 

@@ -72,6 +72,26 @@ class ExArgs(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("chain", C.c_uint32), ("flags", C.c_uint32)]
 
 
+class Problem(C.Structure):
+    """GpuldaProblem of include/gpulda_batch.h."""
+    _fields_ = [
+        ("alpha", C.c_float), ("beta", C.c_float), ("K", C.c_uint32), ("V", C.c_uint32),
+        ("C", C.c_void_p), ("z", C.c_void_p), ("w", C.c_void_p), ("d_len", C.c_void_p),
+        ("n_tokens", C.c_uint64), ("n_docs", C.c_uint32), ("flags", C.c_uint32),
+        ("seed", C.c_uint64), ("chain", C.c_uint32), ("reserved", C.c_uint32),
+    ]
+
+
+class BatchShape(C.Structure):
+    """GpuldaBatchShape of include/gpulda_batch.h."""
+    _fields_ = [("z_warps_per_block", C.c_uint32), ("z_blocks_per_sm", C.c_uint32),
+                ("phi_cells_per_block", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+BATCH_BUCKETS = 4
+BATCH_MAX_K = 2048
+
+assert C.sizeof(Problem) == 80 and C.sizeof(BatchShape) == 16
 assert C.sizeof(Args) == 32 and Args.C.offset == 16
 assert C.sizeof(Buffer) == 96 and Buffer.gpu_z.offset == 40
 
@@ -107,6 +127,19 @@ _SIGNATURES = {
     "gpulda_debug_alias": (C.c_int, [_U32P, C.c_uint32, _U64P]),
     "gpulda_sample_z_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
                                                  C.c_void_p]),
+    # include/gpulda_batch.h
+    "gpulda_batch_create": (C.c_int, [C.POINTER(Problem), C.c_uint32, C.POINTER(C.c_void_p)]),
+    "gpulda_batch_destroy": (C.c_int, [C.c_void_p]),
+    "gpulda_batch_sweep": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "gpulda_batch_sweep_async": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
+    "gpulda_batch_sync": (C.c_int, [C.c_void_p]),
+    "gpulda_batch_read_z": (C.c_int, [C.c_void_p, C.c_uint32, _U32P]),
+    "gpulda_batch_read_counts": (C.c_int, [C.c_void_p, C.c_uint32, _U32P]),
+    "gpulda_batch_loglik": (C.c_int, [C.c_void_p, _F64P, _U64P]),
+    "gpulda_batch_get_shapes": (C.c_int, [C.c_void_p, C.POINTER(BatchShape)]),
+    "gpulda_batch_set_shapes": (C.c_int, [C.c_void_p, C.POINTER(BatchShape)]),
+    "gpulda_batch_tune": (C.c_int, [C.c_void_p, C.c_char_p, _U32P]),
+    "gpulda_batch_info": (C.c_int, [C.c_void_p, _U64P, C.c_int]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGNATURES)

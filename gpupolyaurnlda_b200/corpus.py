@@ -174,6 +174,23 @@ def generate(wl: Workload | str, seed: int = 1, device: str = "cpu", D: int | No
                   z_true=to(z_true))
 
 
+def batched_workloads(n: int = 64, seed: int = 1, D_scale: float = 1.0) -> list[Workload]:
+    """The batched-chains workload: n independent problems with K drawn from
+    {50, 200, 1000}, V from [5000, 50000], D from [1000, 100000] (times
+    D_scale), document lengths lognormal(4.5, 1.0) clipped to [1, 65535] (the
+    16-bit count width; the clip removes no mass at these parameters), the
+    topic generator of ``mid``, alpha = 50/K, beta = 0.01.  Problem i is then
+    drawn by ``generate(wl[i], seed=seed + 1000 + i)``."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        K = int(rng.choice([50, 200, 1000]))
+        V = int(rng.integers(5000, 50001))
+        D = max(1, int(round(int(rng.integers(1000, 100001)) * D_scale)))
+        out.append(Workload(f"batch{i}", K, V, D, 50.0 / K, 0.01, ("lognormal", 4.5, 1.0, 1, 65535), 1.05))
+    return out
+
+
 # --- reference file formats ----------------------------------------------------
 
 def write_files(c: Corpus, directory: str) -> dict:

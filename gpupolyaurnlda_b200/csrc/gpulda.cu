@@ -290,6 +290,9 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
   CK(cudaMemset(g.status, 0, 4));
   CK(cudaMemset(g.counters, 0, kCtrN * 8));
   CK(cudaMemset(g.ll, 0, 16));
+  // A pageable cudaMemcpy may return before its data lands; kernels on the
+  // library's non-blocking streams must not start before that.
+  CK(cudaDeviceSynchronize());
 
   g.dev.K = g.K;
   g.dev.V = g.V;
@@ -498,6 +501,11 @@ int pipelined_sweep(Buffer* b, BufCtx* ctx) {
 
 }  // namespace
 
+namespace gpulda {
+int report_error(int code, const char* what) { return fail(code, what); }
+int report_cuda_error(cudaError_t e, const char* where) { return cuda_fail(e, where); }
+}  // namespace gpulda
+
 // ---------------------------------------------------------------------------
 // reference ABI
 // ---------------------------------------------------------------------------
@@ -684,6 +692,7 @@ extern "C" int gpulda_corpus_load(const uint32_t* z, const uint32_t* w, const ui
   std::vector<u32> order;
   g.c_split = split_longest_first(d_len, n_docs, order, g.K);
   CK(cudaMemcpy(g.corder, order.data(), (size_t)n_docs * 4, cudaMemcpyHostToDevice));
+  CK(cudaDeviceSynchronize());  // uploads complete before non-blocking streams use them
   launch_doc_offsets(g.cd_len, g.cd_idx, n_docs, g.stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(g.stream));
@@ -763,6 +772,7 @@ extern "C" int gpulda_debug_write_counts(const uint32_t* n) {
   if (!g.live) return fail(GPULDA_ERR_STATE, "debug_write_counts before initialize");
   CK(cudaDeviceSynchronize());
   CK(cudaMemcpy(g.dev.n, n, (size_t)g.K * g.V * 4, cudaMemcpyHostToDevice));
+  CK(cudaDeviceSynchronize());
   return GPULDA_OK;
 }
 

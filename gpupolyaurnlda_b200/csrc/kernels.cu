@@ -24,18 +24,18 @@ namespace {
 // n[w][k] ~ Poisson(beta + floor(C[w] / K)).  One Philox block serves the
 // four cells 4g .. 4g+3.
 // ---------------------------------------------------------------------------
-__global__ void init_counts_kernel(ModelDev m, const u32* __restrict__ C) {
-  const u64 cells = (u64)m.K * m.V;
+__global__ void init_counts_kernel(u32* __restrict__ n, u32 K, u32 V, const u32* __restrict__ C, PoisTables tb,
+                                   double beta, u32 key0, u32 key1) {
+  const u64 cells = (u64)K * V;
   const u64 groups = (cells + 3) / 4;
   for (u64 gi = (u64)blockIdx.x * blockDim.x + threadIdx.x; gi < groups; gi += (u64)gridDim.x * blockDim.x) {
-    const U4 r = draw4(gi, 0, kStreamInitCounts, 0, m.key0, m.key1);
+    const U4 r = draw4(gi, 0, kStreamInitCounts, 0, key0, key1);
 #pragma unroll
     for (u32 u = 0; u < 4; ++u) {
       const u64 c = gi * 4 + u;
       if (c < cells) {
-        const u32 lam_n = C[c / m.K] / m.K;
-        m.n[c] = poisson_draw(lam_n, (double)m.beta, u4_word(r, u), c, 0, kStreamInitCounts, m.key0, m.key1,
-                              m.tables);
+        const u32 lam_n = C[c / K] / K;
+        n[c] = poisson_draw(lam_n, beta, u4_word(r, u), c, 0, kStreamInitCounts, key0, key1, tb);
       }
     }
   }
@@ -48,6 +48,53 @@ __global__ void init_counts_kernel(ModelDev m, const u32* __restrict__ C) {
 // stores when the group lies inside the range).  Per-topic sums are gathered
 // in shared memory (integer atomics: order-free) and flushed once per block.
 // ---------------------------------------------------------------------------
+// Cells [c0, c1) of one model (local cell indices; n and q point at its cell
+// 0).  Nonzero draws are added to the per-topic sums: into shared memory when
+// s_sum is given, else straight into S.
+__device__ __forceinline__ void phi_rows(u32 K, u64 c0, u64 c1, u32* __restrict__ n, u32* __restrict__ q, u64* S,
+                                         const PoisTables& tb, double beta, u32 key0, u32 key1, u32 t,
+                                         unsigned long long* s_sum) {
+  for (u64 gi = c0 / 4 + threadIdx.x; gi * 4 < c1; gi += blockDim.x) {
+    const u64 cb = gi * 4;
+    const U4 r = draw4(gi, t, kStreamPhi, 0, key0, key1);
+    const bool whole = cb >= c0 && cb + 4 <= c1;
+    u32 nv[4];
+    if (whole) {
+      const uint4 v = *reinterpret_cast<const uint4*>(n + cb);
+      nv[0] = v.x;
+      nv[1] = v.y;
+      nv[2] = v.z;
+      nv[3] = v.w;
+    } else {
+#pragma unroll
+      for (u32 u = 0; u < 4; ++u) nv[u] = (cb + u >= c0 && cb + u < c1) ? n[cb + u] : 0u;
+    }
+    u32 xv[4];
+#pragma unroll
+    for (u32 u = 0; u < 4; ++u) xv[u] = poisson_draw(nv[u], beta, u4_word(r, u), cb + u, t, kStreamPhi, key0, key1, tb);
+    if (whole) {
+      *reinterpret_cast<uint4*>(q + cb) = make_uint4(xv[0], xv[1], xv[2], xv[3]);
+      *reinterpret_cast<uint4*>(n + cb) = make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (u32 u = 0; u < 4; ++u) {
+      const u64 c = cb + u;
+      if (c < c0 || c >= c1) continue;
+      if (!whole) {
+        q[c] = xv[u];
+        n[c] = 0;
+      }
+      if (xv[u]) {
+        const u32 k = (u32)(c % K);
+        if (s_sum)
+          atomicAdd(&s_sum[k], (unsigned long long)xv[u]);
+        else
+          atomicAdd((unsigned long long*)&S[k], (unsigned long long)xv[u]);
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256) phi_draw_kernel(ModelDev m, u32 t, u32 rows_per_block, int smem_sums) {
   extern __shared__ unsigned long long s_sum[];
   const u32 K = m.K;
@@ -57,55 +104,31 @@ __global__ void __launch_bounds__(256) phi_draw_kernel(ModelDev m, u32 t, u32 ro
   }
   const u32 w0 = blockIdx.x * rows_per_block;
   const u32 w1 = min(m.V, w0 + rows_per_block);
-  const u64 c0 = (u64)w0 * K, c1 = (u64)w1 * K;
-  const double beta = (double)m.beta;
-  for (u64 gi = c0 / 4 + threadIdx.x; gi * 4 < c1; gi += blockDim.x) {
-    const u64 cb = gi * 4;
-    const U4 r = draw4(gi, t, kStreamPhi, 0, m.key0, m.key1);
-    const bool whole = cb >= c0 && cb + 4 <= c1;
-    u32 nv[4];
-    if (whole) {
-      const uint4 v = *reinterpret_cast<const uint4*>(m.n + cb);
-      nv[0] = v.x;
-      nv[1] = v.y;
-      nv[2] = v.z;
-      nv[3] = v.w;
-    } else {
-#pragma unroll
-      for (u32 u = 0; u < 4; ++u) nv[u] = (cb + u >= c0 && cb + u < c1) ? m.n[cb + u] : 0u;
-    }
-    u32 xv[4];
-#pragma unroll
-    for (u32 u = 0; u < 4; ++u) {
-      const u64 c = cb + u;
-      xv[u] = poisson_draw(nv[u], beta, u4_word(r, u), c, t, kStreamPhi, m.key0, m.key1, m.tables);
-    }
-    if (whole) {
-      *reinterpret_cast<uint4*>(m.q + cb) = make_uint4(xv[0], xv[1], xv[2], xv[3]);
-      *reinterpret_cast<uint4*>(m.n + cb) = make_uint4(0, 0, 0, 0);
-    }
-#pragma unroll
-    for (u32 u = 0; u < 4; ++u) {
-      const u64 c = cb + u;
-      if (c < c0 || c >= c1) continue;
-      if (!whole) {
-        m.q[c] = xv[u];
-        m.n[c] = 0;
-      }
-      if (xv[u]) {
-        const u32 k = (u32)(c % K);
-        if (smem_sums)
-          atomicAdd(&s_sum[k], (unsigned long long)xv[u]);
-        else
-          atomicAdd((unsigned long long*)&m.S[k], (unsigned long long)xv[u]);
-      }
-    }
-  }
+  phi_rows(K, (u64)w0 * K, (u64)w1 * K, m.n, m.q, m.S, m.tables, (double)m.beta, m.key0, m.key1, t,
+           smem_sums ? s_sum : nullptr);
   if (smem_sums) {
     __syncthreads();
     for (u32 k = threadIdx.x; k < K; k += blockDim.x)
       if (s_sum[k]) atomicAdd((unsigned long long*)&m.S[k], s_sum[k]);
   }
+}
+
+// Batched Phi draw: block b draws rows [w0, w1) (problem-local word ids) of
+// problem p, with (p, w0, w1) from the block table.
+__global__ void __launch_bounds__(256) phi_draw_batch_kernel(ModelDev ar, BatchPhiDev bp, const u32* t_dev) {
+  extern __shared__ unsigned long long s_sum[];
+  const uint4 e = bp.blocks[blockIdx.x];
+  const u32 pb = e.x, K = bp.K[pb];
+  for (u32 k = threadIdx.x; k < K; k += blockDim.x) s_sum[k] = 0;
+  __syncthreads();
+  const u64 cell0 = bp.cell_base[pb];
+  PoisTables tb{bp.cdf + (size_t)pb * kPoisN * kPoisW, bp.guide + (size_t)pb * kPoisN * 256, bp.lfac + (size_t)pb * kLogFacN};
+  u64* S = ar.S + bp.S_off[pb];
+  phi_rows(K, (u64)e.y * K, (u64)e.z * K, ar.n + cell0, ar.q + cell0, S, tb, (double)bp.beta[pb], bp.key0[pb],
+           bp.key1[pb], *t_dev, s_sum);
+  __syncthreads();
+  for (u32 k = threadIdx.x; k < K; k += blockDim.x)
+    if (s_sum[k]) atomicAdd((unsigned long long*)&S[k], s_sum[k]);
 }
 
 // ---------------------------------------------------------------------------
@@ -198,6 +221,41 @@ __device__ void alias_build_block(const u64* wq, const uint16_t* key, u32 n, u64
 // list q << 32 | k, the dense mass A) and the sparse alias table over them.
 // Persistent blocks loop over words; scratch is shared memory or, for large
 // K, a per-block slice of global memory.
+__device__ __forceinline__ void alias_word(u32 K, u32* __restrict__ qrow, const u64* __restrict__ S, u64* alrow,
+                                           u64* csrrow, u64* A_out, u32* nnz_out, u64* cq, u64* vals, uint16_t* ck,
+                                           uint16_t* idx, u64* sh) {
+  u64 part = 0, nz = 0;
+  for (u32 t0 = 0; t0 < K; t0 += blockDim.x) {
+    const u32 k = t0 + threadIdx.x;
+    u64 qq = 0;
+    if (k < K) {
+      const u32 x = qrow[k];
+      if (x) {
+        qq = (((u64)x) << 32) / S[k];
+        if (qq > 0xffffffffULL) qq = 0xffffffffULL;
+      }
+      qrow[k] = (u32)qq;
+    }
+    u64 tile;
+    const u64 pos = nz + block_excl_scan_u64(qq != 0, sh, &tile);
+    if (qq) {
+      cq[pos] = qq;
+      ck[pos] = (uint16_t)k;
+    }
+    nz += tile;
+    part += qq;
+  }
+  const u64 A = block_sum_u64(part, sh);  // (also a barrier for cq/ck)
+  const u32 n = (u32)nz;
+  for (u32 i = threadIdx.x; i < n; i += blockDim.x) csrrow[i] = (cq[i] << 32) | ck[i];
+  if (n) alias_build_block(cq, ck, n, A, vals, idx, alrow, sh);
+  if (threadIdx.x == 0) {
+    *A_out = A;
+    *nnz_out = n;
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(256) alias_build_kernel(ModelDev m, unsigned char* gscratch, size_t slice) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   __shared__ u64 sh[33];
@@ -209,38 +267,29 @@ __global__ void __launch_bounds__(256) alias_build_kernel(ModelDev m, unsigned c
   uint16_t* idx = ck + K;
   for (u32 w = blockIdx.x; w < m.V; w += gridDim.x) {
     const size_t row = (size_t)w * K;
-    u64 part = 0, nz = 0;
-    for (u32 t0 = 0; t0 < K; t0 += blockDim.x) {
-      const u32 k = t0 + threadIdx.x;
-      u64 qq = 0;
-      if (k < K) {
-        const u32 x = m.q[row + k];
-        if (x) {
-          qq = (((u64)x) << 32) / m.S[k];
-          if (qq > 0xffffffffULL) qq = 0xffffffffULL;
-        }
-        m.q[row + k] = (u32)qq;
-      }
-      u64 tile;
-      const u64 pos = nz + block_excl_scan_u64(qq != 0, sh, &tile);
-      if (qq) {
-        cq[pos] = qq;
-        ck[pos] = (uint16_t)k;
-      }
-      nz += tile;
-      part += qq;
-    }
-    const u64 A = block_sum_u64(part, sh);  // (also a barrier for cq/ck)
-    const u32 n = (u32)nz;
-    for (u32 i = threadIdx.x; i < n; i += blockDim.x) m.csr[row + i] = (cq[i] << 32) | ck[i];
-    if (n) alias_build_block(cq, ck, n, A, vals, idx, m.al + row, sh);
-    if (threadIdx.x == 0) {
-      m.A[w] = A;
-      m.nnz[w] = n;
-    }
-    __syncthreads();
+    alias_word(K, m.q + row, m.S, m.al + row, m.csr + row, m.A + w, m.nnz + w, cq, vals, ck, idx, sh);
   }
 }
+
+// Batched alias build over global words [w0, w1) of any problems; shared
+// memory sized for the largest K among them.
+__global__ void __launch_bounds__(256) alias_build_batch_kernel(ModelDev ar, BatchPhiDev bp, u32 Kmax, u32 w0, u32 w1) {
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  __shared__ u64 sh[33];
+  u64* cq = (u64*)s_raw;
+  u64* vals = cq + Kmax;
+  uint16_t* ck = (uint16_t*)(vals + Kmax);
+  uint16_t* idx = ck + Kmax;
+  for (u32 w = w0 + blockIdx.x; w < w1; w += gridDim.x) {
+    const u32 pb = bp.wpid[w], K = bp.K[pb];
+    const size_t row = bp.row_off[w];
+    alias_word(K, ar.q + row, ar.S + bp.S_off[pb], ar.al + row, ar.csr + row, ar.A + w, ar.nnz + w, cq, vals, ck,
+               idx, sh);
+  }
+}
+
+// Advances a device-side iteration counter (replayed graphs read it).
+__global__ void bump_kernel(u32* t) { *t += 1; }
 
 __global__ void debug_alias_kernel(const u32* q, u32 K, u64* out) {
   extern __shared__ __align__(16) unsigned char s_raw[];
@@ -299,6 +348,9 @@ __global__ void debug_poisson_kernel(ModelDev m, const u32* count, const u64* id
 
 }  // namespace
 
+static u32 alias_threads(u32 K);
+static size_t alias_smem_bytes(u32 K);
+
 int device_sm_count() {
   static int sms = 0;
   if (!sms) {
@@ -311,10 +363,37 @@ int device_sm_count() {
 }
 
 void launch_init_counts(const ModelDev& m, const u32* C, cudaStream_t s) {
-  const u64 cells = (u64)m.K * m.V;
-  const u32 blocks = (u32)std::min<u64>((cells + 255) / 256, (u64)device_sm_count() * 16);
-  init_counts_kernel<<<blocks, 256, 0, s>>>(m, C);
+  launch_init_counts_raw(m.n, m.K, m.V, C, m.tables, m.beta, m.key0, m.key1, s);
 }
+
+void launch_init_counts_raw(u32* n, u32 K, u32 V, const u32* C, const PoisTables& tb, float beta, u32 key0, u32 key1,
+                            cudaStream_t s) {
+  const u64 groups = ((u64)K * V + 3) / 4;
+  const u32 blocks = (u32)std::max<u64>(1, std::min<u64>((groups + 255) / 256, (u64)device_sm_count() * 16));
+  init_counts_kernel<<<blocks, 256, 0, s>>>(n, K, V, C, tb, (double)beta, key0, key1);
+}
+
+void launch_phi_draw_batch(const ModelDev& ar, const BatchPhiDev& bp, u32 n_blocks, u32 Kmax, const u32* t_dev,
+                           cudaStream_t s) {
+  if (!n_blocks) return;
+  const size_t smem = (size_t)Kmax * 8;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(phi_draw_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  phi_draw_batch_kernel<<<n_blocks, 256, smem, s>>>(ar, bp, t_dev);
+}
+
+void launch_alias_build_batch(const ModelDev& ar, const BatchPhiDev& bp, u32 Kmax, u32 w0, u32 w1, cudaStream_t s) {
+  if (w1 <= w0) return;
+  const u32 nt = alias_threads(Kmax);
+  const size_t need = alias_smem_bytes(Kmax);
+  if (need > 48 * 1024) cudaFuncSetAttribute(alias_build_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, alias_build_batch_kernel, nt, need);
+  if (per_sm < 1) per_sm = 1;
+  const u32 blocks = std::min<u32>(w1 - w0, (u32)(device_sm_count() * per_sm * 4));
+  alias_build_batch_kernel<<<blocks, nt, need, s>>>(ar, bp, Kmax, w0, w1);
+}
+
+void launch_bump(u32* t, cudaStream_t s) { bump_kernel<<<1, 1, 0, s>>>(t); }
 
 void launch_phi_draw(const ModelDev& m, u32 t, cudaStream_t s) {
   const u32 rows = std::max<u32>(1u, 65536u / m.K);

@@ -37,6 +37,8 @@ constexpr size_t kZMaxSmem = 200 * 1024;
 struct ZKernelArgs {
   ModelDev m;
   ZLaunch z;
+  BatchDev b;    // problem tables (batched launches only)
+  u32 Kmax;      // largest K of the launch (sets the shared-memory stride)
   double lg_Ka;  // lgamma(K * alpha)
   double lg_a;   // lgamma(alpha)
 };
@@ -97,19 +99,24 @@ __host__ __device__ __forceinline__ size_t z_warp_bytes(u32 K) {
   return Kp * 4 + ((Kp / 8 + 15) & ~(size_t)15);
 }
 
+// BATCH: the launch sweeps documents of many independent problems laid out in
+// one set of arenas; each document's K, alpha, Philox key and token numbering
+// come from its problem, and a token's (word, topic) row starts at
+// b.row_off[w] instead of w * K.  Otherwise all parameters come from `m`.
+template <bool BATCH>
 __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
   extern __shared__ __align__(16) unsigned char zsm[];
   const ModelDev& m = a.m;
   const ZLaunch& p = a.z;
   const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const u32 K = m.K, V = m.V;
-  const u32 Kp = (K + 63) & ~63u;
-  uint16_t* cnt = (uint16_t*)(zsm + (size_t)warp * z_warp_bytes(K));
+  const u32 V = m.V;
+  const u32 Kpmax = (a.Kmax + 63) & ~63u;
+  uint16_t* cnt = (uint16_t*)(zsm + (size_t)warp * z_warp_bytes(a.Kmax));
   // Sorted topics of the document: every topic with a nonzero count, plus
   // topics whose count fell to zero since the last compaction (their mass is
   // zero, so they never change B or the selected topic).
-  uint16_t* tl = cnt + Kp;
-  u32* inl = (u32*)(tl + Kp);  // bitmap: topic is in tl
+  uint16_t* tl = cnt + Kpmax;
+  u32* inl = (u32*)(tl + Kpmax);  // bitmap: topic is in tl
   const bool want_ll = (p.flags & 1u) && p.ll;
 
   u64 st_tok = 0, st_docs = 0, st_S = 0, st_sp = 0;
@@ -124,6 +131,23 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
     if (p.order) doc = p.order[doc];
     const u32 L = p.d_len[doc];
     const u64 off = p.d_idx[doc];
+    u32 K = m.K, key0 = m.key0, key1 = m.key1, pb = 0;
+    float alpha = m.alpha;
+    u64 tok_base = p.tok_base;
+    double lg_a = a.lg_a, lg_Ka = a.lg_Ka;
+    const u32* __restrict__ t_ptr = p.t_dev;
+    if (BATCH) {
+      pb = a.b.pid[doc];
+      K = a.b.K[pb];
+      alpha = a.b.alpha[pb];
+      key0 = a.b.key0[pb];
+      key1 = a.b.key1[pb];
+      tok_base = a.b.tok_base[pb];  // the problem's first token: local numbering
+      lg_a = a.b.lg_a[pb];
+      lg_Ka = a.b.lg_Ka[pb];
+    }
+    const u32 t = t_ptr ? *t_ptr : p.t;
+    const u32 Kp = (K + 63) & ~63u;
     if (L > kMaxDocLen) {
       status |= kStatusDocTooLong;
       continue;
@@ -178,7 +202,9 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
         my_w %= V;
       }
       if (my_z >= K) my_z %= K;
-      const U4 r = draw4(p.tok_base + off + i, p.t, kStreamZ, 0, m.key0, m.key1);
+      // Philox index: the token's position in its corpus (batched problems
+      // count from their own first token) plus the buffer's offset.
+      const U4 r = draw4(BATCH ? off + i - tok_base : tok_base + off + i, t, kStreamZ, 0, key0, key1);
       // Per-token word data for the whole chunk, loaded lane-parallel so the
       // token loop never waits on them: nnz, dense mass, and the alias entry
       // of the slot this token's dense draw would use.
@@ -186,7 +212,8 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
       const u32 my_nw = valid ? __ldg(m.nnz + my_w) : 0u;
       const u64 my_A = valid ? __ldg(m.A + my_w) : 0ull;
       const u32 my_s = (u32)(((u64)r.z * my_nw) >> 32);
-      const u64 my_al = (valid && my_nw) ? __ldg(m.al + (size_t)my_w * K + my_s) : 0ull;
+      const u64 my_row = BATCH ? (valid ? __ldg(a.b.row_off + my_w) : 0ull) : (u64)my_w * K;
+      const u64 my_al = (valid && my_nw) ? __ldg(m.al + my_row + my_s) : 0ull;
       u32 new_z = my_z;
       const u32 nt = min(32u, L - base);
       for (u32 j = 0; j < nt; ++j) {
@@ -194,7 +221,7 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
         const u32 zj = __shfl_sync(kFullMask, my_z, j);
         const u32 r0 = __shfl_sync(kFullMask, r.x, j);
         const u32 r1 = __shfl_sync(kFullMask, r.y, j);
-        const size_t row = (size_t)wj * K;
+        const size_t row = BATCH ? (size_t)__shfl_sync(kFullMask, my_row, j) : (size_t)wj * K;
         const u32* __restrict__ qrow = m.q + row;
         const u64* __restrict__ crow = m.csr + row;
         const u32 nw = __shfl_sync(kFullMask, my_nw, j);
@@ -225,7 +252,7 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
         const u64 incl = warp_incl_scan_u64(ls, lane);
         const u64 B = __shfl_sync(kFullMask, incl, 31);
         int degenerate;
-        const int sp = take_sparse(r0, m.alpha, Aw, B, &degenerate);
+        const int sp = take_sparse(r0, alpha, Aw, B, &degenerate);
         u32 k = zj;
         if (!degenerate) {
           if (sp) {
@@ -299,10 +326,17 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
       double dl = 0.0;
       for (u32 e = lane; e < nl; e += 32) {
         const u32 c = cnt[tl[e]];
-        if (c) dl += lgamma((double)m.alpha + (double)c) - a.lg_a;
+        if (c) dl += lgamma((double)alpha + (double)c) - lg_a;
       }
       dl = warp_sum_f64(dl);
-      if (lane == 0) ll_acc += dl + a.lg_Ka - lgamma((double)K * (double)m.alpha + (double)L);
+      if (lane == 0) ll_acc += dl + lg_Ka - lgamma((double)K * (double)alpha + (double)L);
+      if (BATCH) {  // per-problem sums
+        if (lane == 0) {
+          atomicAdd(p.ll + 2 * pb, ll_acc);
+          atomicAdd(p.ll + 2 * pb + 1, ll_skip);
+        }
+        ll_acc = ll_skip = 0.0;
+      }
     }
     st_tok += L;
     st_docs += 1;
@@ -313,13 +347,33 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
     atomicAdd(p.counters + kCtrDocs, (unsigned long long)st_docs);
     atomicAdd(p.counters + kCtrSparseWork, (unsigned long long)st_S);
     atomicAdd(p.counters + kCtrSparseDraws, (unsigned long long)st_sp);
-    if (want_ll) {
+    if (want_ll && !BATCH) {
       atomicAdd(p.ll, ll_acc);
       atomicAdd(p.ll + 1, ll_skip);
     }
   }
   status = __reduce_or_sync(kFullMask, status);
   if (lane == 0 && status) atomicOr(p.status, status);
+}
+
+template <bool BATCH>
+void launch_impl(const ZKernelArgs& a, u32 n_docs, cudaStream_t s, u32 wpb, u32 blocks_per_sm) {
+  const size_t per_warp = z_warp_bytes(a.Kmax);
+  // Warps per block: as many as fit the shared-memory budget (at most the request).
+  while (wpb > 1 && per_warp * wpb > kZMaxSmem) --wpb;
+  const size_t smem = per_warp * wpb;
+  // The ceiling, not this launch's size: captured graphs may hold launches of
+  // several sizes.
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(z_sweep_kernel<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZMaxSmem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, z_sweep_kernel<BATCH>, 32 * wpb, smem);
+  if (per_sm < 1) per_sm = 1;
+  if (blocks_per_sm && (int)blocks_per_sm < per_sm) per_sm = (int)blocks_per_sm;
+  u32 blocks = (u32)(device_sm_count() * per_sm);
+  const u32 need = (n_docs + wpb - 1) / wpb;
+  if (blocks > need) blocks = need;
+  z_sweep_kernel<BATCH><<<blocks, 32 * wpb, smem, s>>>(a);
 }
 
 }  // namespace
@@ -331,21 +385,24 @@ void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s) {
   ZKernelArgs a;
   a.m = m;
   a.z = z;
+  a.b = BatchDev{};
+  a.Kmax = m.K;
   a.lg_a = std::lgamma((double)m.alpha);
   a.lg_Ka = std::lgamma((double)m.K * (double)m.alpha);
-  const size_t per_warp = z_sweep_smem_per_warp(m.K);
-  // Warps per block: as many as fit the shared-memory budget, at most 8.
-  u32 wpb = 8;
-  while (wpb > 1 && per_warp * wpb > kZMaxSmem) --wpb;
-  const size_t smem = per_warp * wpb;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(z_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, z_sweep_kernel, 32 * wpb, smem);
-  if (per_sm < 1) per_sm = 1;
-  u32 blocks = (u32)(device_sm_count() * per_sm);
-  const u32 need = (z.n_docs + wpb - 1) / wpb;
-  if (blocks > need) blocks = need;
-  z_sweep_kernel<<<blocks, 32 * wpb, smem, s>>>(a);
+  launch_impl<false>(a, z.n_docs, s, 8, 0);
+}
+
+void launch_z_sweep_batch(const ModelDev& arenas, const BatchDev& b, u32 Kmax, const ZLaunch& z, cudaStream_t s,
+                          u32 warps_per_block, u32 blocks_per_sm) {
+  if (!z.n_docs) return;
+  ZKernelArgs a;
+  a.m = arenas;
+  a.z = z;
+  a.b = b;
+  a.Kmax = Kmax;
+  a.lg_a = 0;
+  a.lg_Ka = 0;
+  launch_impl<true>(a, z.n_docs, s, warps_per_block, blocks_per_sm);
 }
 
 }  // namespace gpulda

@@ -1,6 +1,6 @@
 """CPU-only checks of the drop-in boundary and the host logic (no GPU calls).
 
-* libGPUPolyaUrnLDA.so loads and exports every entry point include/gpulda.h
+* libGPUPolyaUrnLDA.so loads and exports every entry point include/*.h
   declares, with the reference's unmangled names (src/cu/train.cuh:41-45).
 * Args / Buffer layouts equal the reference's repr(C) structs
   (src/ffi.rs:4-13, src/buffer.rs:4-19).
@@ -24,9 +24,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _header_functions():
-    text = open(os.path.join(ROOT, "include", "gpulda.h")).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    names = re.findall(r"^\s*(?:void|int|const char\*)\s+\*?(\w+)\s*\(", text, flags=re.M)
+    names = []
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"^\s*(?:void|int|const char\*)\s+\*?(\w+)\s*\(", text, flags=re.M)
     return names
 
 
@@ -41,7 +45,7 @@ def test_library_exports_every_declared_symbol(built):
     names = _header_functions()
     assert {"initialize", "sample_phi", "sample_z_async", "sync_buffer", "cleanup"} <= set(names)
     for n in names:
-        assert hasattr(built, n), f"{n} declared in include/gpulda.h but not exported"
+        assert hasattr(built, n), f"{n} declared in include/ but not exported"
     assert set(names) == set(g.EXPORTED_SYMBOLS)
 
 
@@ -130,3 +134,39 @@ def test_gpulda_train_binary_parses_reference_flags(built):
     assert os.path.exists(exe)
     r = subprocess.run([exe, "--no_such_flag"], capture_output=True, text=True)
     assert r.returncode == 2 and "unknown flag" in r.stderr
+
+
+def test_batch_problem_layout():
+    # GpuldaProblem of include/gpulda_batch.h
+    P = g.Problem
+    assert C.sizeof(P) == 80
+    assert [P.alpha.offset, P.beta.offset, P.K.offset, P.V.offset, P.C.offset, P.z.offset, P.w.offset,
+            P.d_len.offset, P.n_tokens.offset, P.n_docs.offset, P.flags.offset, P.seed.offset,
+            P.chain.offset] == [0, 4, 8, 12, 16, 24, 32, 40, 48, 56, 60, 64, 72]
+
+
+def test_batch_create_rejects_bad_problems_before_any_device_call(built):
+    """Validation runs on the host before anything touches a device, so the
+    rejected cases need no GPU."""
+    from gpupolyaurnlda_b200.batch import BatchChains, ProblemSpec
+    counts = np.array([3, 2, 1], np.uint32)
+    ok = dict(alpha=0.1, beta=0.01, K=4, counts=counts, z=np.array([0, 1, 2], np.uint32),
+              w=np.array([0, 1, 2], np.uint32), d_len=np.array([2, 1], np.uint32))
+    cases = [
+        (dict(K=4096), 7),                                        # above GPULDA_BATCH_MAX_K
+        (dict(K=0), 2),
+        (dict(alpha=0.0), 2),
+        (dict(w=np.array([0, 1, 3], np.uint32)), 2),              # word id >= V
+        (dict(z=np.array([0, 1, 4], np.uint32)), 2),              # topic >= K
+        (dict(d_len=np.array([2, 2], np.uint32)), 2),             # lengths do not sum to n_tokens
+        (dict(d_len=np.array([70000], np.uint32), z=np.zeros(70000, np.uint32),
+              w=np.zeros(70000, np.uint32)), 7),                  # document above GPULDA_MAX_DOC_LEN
+    ]
+    for change, code in cases:
+        spec = ProblemSpec(**{**ok, **change})
+        with pytest.raises(GpuldaError) as e:
+            BatchChains([ProblemSpec(**ok), spec])
+        assert e.value.code == code, change
+    with pytest.raises(GpuldaError) as e:
+        BatchChains([])
+    assert e.value.code == 2
