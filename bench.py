@@ -52,6 +52,12 @@ def parse():
     p.add_argument("--problems", type=int, default=64, help="batched workload: number of problems")
     p.add_argument("--batch-scale", type=float, default=1.0, help="batched workload: scale of each problem's D")
     p.add_argument("--tune-cache", default=None, help="batched workload: autotuner cache file")
+    p.add_argument("--rates", type=int, nargs="+", default=[1000, 10000, 50000], help="serve: offered docs/s")
+    p.add_argument("--serve-requests", type=int, default=100000, help="serve: max requests per rate")
+    p.add_argument("--serve-seconds", type=float, default=2.0, help="serve: seconds of arrivals per rate")
+    p.add_argument("--serve-unbatched", type=int, default=3000, help="serve: requests of the unbatched run")
+    p.add_argument("--serve-train", type=int, default=5, help="serve: training iterations of the model")
+    p.add_argument("--serve-slots", type=int, default=32, help="serve: launches in flight")
     return p.parse_args()
 
 
@@ -456,12 +462,129 @@ def run_batched(args):
         dist.destroy_process_group()
 
 
+def serve_open_loop(srv, lengths, words, arrival_s, ids):
+    """Submits requests at their arrival times (open loop), keeps the server
+    progressing and collects results.  Returns docs/s (requests over the time
+    from the first arrival to the last completion), latencies (ns, completion
+    minus scheduled arrival) and per-request log-likelihoods and skipped
+    counts, in request order."""
+    n = len(lengths)
+    offs = np.concatenate([[0], np.cumsum(lengths.astype(np.int64))])
+    t0 = time.monotonic_ns() + 2_000_000
+    arr = t0 + (arrival_s * 1e9).astype(np.int64)
+    lat = np.zeros(n, np.int64)
+    ll = np.zeros(n, np.float64)
+    sk = np.zeros(n, np.int64)
+    seen = np.zeros(n, bool)
+    i = done = 0
+    last = 0
+    while done < n:
+        now = time.monotonic_ns()
+        j = int(np.searchsorted(arr, now, side="right"))
+        busy = False
+        if j > i:
+            srv.submit(ids[i:j], lengths[i:j], words[offs[i]:offs[j]])
+            i = j
+            busy = True
+        srv.progress()
+        out = srv.poll(1 << 16, theta=False)
+        k = len(out["ids"])
+        if k:
+            r = (out["ids"] - ids[0]).astype(np.int64)
+            lat[r] = out["done_ns"].astype(np.int64) - arr[r]
+            ll[r] = out["ll"]
+            sk[r] = out["skipped"]
+            seen[r] = True
+            last = max(last, int(out["done_ns"].max()))
+            done += k
+            busy = True
+        if not busy:
+            time.sleep(2e-5)
+    assert seen.all()
+    return n / ((last - arr[0]) / 1e9), lat, ll, sk
+
+
+def run_serve(args):
+    """Serving fold-in: a K=1000, V=100000 model trained on the mid corpus is
+    served to Poisson arrivals of Zipf documents (lengths lognormal(5.0, 1.2)
+    clipped to [5, 20000]), 50 fold-in iterations each; continuous batching
+    against one launch per document on the same request streams."""
+    import torch
+
+    import gpupolyaurnlda_b200 as g
+    from gpupolyaurnlda_b200 import corpus
+    from gpupolyaurnlda_b200.serve import Server, zipf_requests
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    c = corpus.generate("mid", seed=1, device=f"cuda:{local}")
+    s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=0)
+    s.corpus_load(c.z.copy(), c.w, c.d_len)
+    s.corpus_sweep(args.serve_train)
+    n_iter = 50
+    srv_b = Server(n_iter, seed=0, max_inflight=1 << 17)  # persistent: 32 request warps per SM
+    srv_u = Server(n_iter, mode="launch", slots=args.serve_slots, max_batch=1, seed=0)
+    s.close()
+    del c
+    rows = []
+    ll_b_all, ll_u_all, tok_all = [], [], []
+    for rate in args.rates:
+        n = int(min(max(args.serve_seconds * rate, 2000), args.serve_requests))
+        lengths, words = zipf_requests(n, srv_b.V, seed=rate)
+        rng = np.random.default_rng(rate + 1)
+        arrival = np.cumsum(rng.exponential(1.0 / rate, n))
+        ids = np.arange(n, dtype=np.uint64) + np.uint64(rate) * np.uint64(1 << 32)
+        clocks = ClockSampler(local)
+        clocks.start()
+        dps_b, lat_b, ll_b, sk_b = serve_open_loop(srv_b, lengths, words, arrival, ids)
+        clk = clocks.stop()
+        nu = min(n, args.serve_unbatched)
+        dps_u, lat_u, ll_u, sk_u = serve_open_loop(srv_u, lengths[:nu], words[:int(lengths[:nu].sum())],
+                                                   arrival[:nu], ids[:nu])
+        same = bool((ll_b[:nu] == ll_u).all() and (sk_b[:nu] == sk_u).all())
+        ll_b_all.append(ll_b[:nu].sum())
+        ll_u_all.append(ll_u.sum())
+        tok_all.append(float((lengths[:nu].astype(np.int64) - sk_u).sum()))
+        rows.append({"offered_docs_per_sec": rate, "requests": n, "tokens": int(lengths.sum()),
+                     "batched": {"docs_per_sec": dps_b, "p50_ms": float(np.percentile(lat_b, 50) / 1e6),
+                                 "p99_ms": float(np.percentile(lat_b, 99) / 1e6)},
+                     "unbatched": {"requests": nu, "docs_per_sec": dps_u,
+                                   "p50_ms": float(np.percentile(lat_u, 50) / 1e6),
+                                   "p99_ms": float(np.percentile(lat_u, 99) / 1e6)},
+                     "results_identical": same, "clocks": clk})
+    st_b = srv_b.stats()
+    srv_b.close()
+    srv_u.close()
+    top = rows[-1]
+    llb, llu = sum(ll_b_all) / sum(tok_all), sum(ll_u_all) / sum(tok_all)
+    if rank == 0:
+        line = {"metric": "served_docs_per_sec", "value": top["batched"]["docs_per_sec"], "unit": "docs/s",
+                "n_gpus": 1, "steps": len(rows), "warmup": 0,
+                "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u64", "data": "synthetic",
+                "config": {"workload": f"serving fold-in: K=1000 V=100000 model (mid corpus, {args.serve_train} "
+                                       f"training iterations), {n_iter} fold-in iterations per request, Zipf(1.05) "
+                                       f"documents, lengths lognormal(5.0,1.2) clipped [5,20000], Poisson arrivals "
+                                       f"at {list(args.rates)} docs/s",
+                           "batched": "persistent kernel, 32 request warps per SM",
+                           "unbatched": f"one launch per document, {args.serve_slots} streams"},
+                "p50_ms": top["batched"]["p50_ms"], "p99_ms": top["batched"]["p99_ms"],
+                "unbatched": top["unbatched"],
+                "speedup_vs_unbatched": top["batched"]["docs_per_sec"] / top["unbatched"]["docs_per_sec"],
+                "heldout_ll_per_token": {"batched": llb, "unbatched": llu, "rel_diff": abs(llb - llu) / abs(llu)},
+                "rates": rows, "server_stats": st_b}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

@@ -88,10 +88,21 @@ class BatchShape(C.Structure):
                 ("phi_cells_per_block", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class ServeArgs(C.Structure):
+    """GpuldaServeArgs of include/gpulda_serve.h."""
+    _fields_ = [("n_iter", C.c_uint32), ("mode", C.c_uint32), ("slots", C.c_uint32), ("max_batch", C.c_uint32),
+                ("max_inflight", C.c_uint32), ("chain", C.c_uint32), ("seed", C.c_uint64),
+                ("pool_bytes", C.c_uint64)]
+
+
+SERVE_PERSISTENT = 0
+SERVE_LAUNCH = 1
+
+
 BATCH_BUCKETS = 4
 BATCH_MAX_K = 2048
 
-assert C.sizeof(Problem) == 80 and C.sizeof(BatchShape) == 16
+assert C.sizeof(Problem) == 80 and C.sizeof(BatchShape) == 16 and C.sizeof(ServeArgs) == 40
 assert C.sizeof(Args) == 32 and Args.C.offset == 16
 assert C.sizeof(Buffer) == 96 and Buffer.gpu_z.offset == 40
 
@@ -140,6 +151,16 @@ _SIGNATURES = {
     "gpulda_batch_set_shapes": (C.c_int, [C.c_void_p, C.POINTER(BatchShape)]),
     "gpulda_batch_tune": (C.c_int, [C.c_void_p, C.c_char_p, _U32P]),
     "gpulda_batch_info": (C.c_int, [C.c_void_p, _U64P, C.c_int]),
+    # include/gpulda_serve.h
+    "gpulda_serve_create": (C.c_int, [C.POINTER(ServeArgs), C.POINTER(C.c_void_p)]),
+    "gpulda_serve_create_from_phi": (C.c_int, [C.POINTER(ServeArgs), C.c_uint32, C.c_uint32, C.c_float, _U32P,
+                                               C.POINTER(C.c_void_p)]),
+    "gpulda_serve_destroy": (C.c_int, [C.c_void_p]),
+    "gpulda_serve_submit": (C.c_int, [C.c_void_p, C.c_uint32, _U64P, _U32P, _U32P]),
+    "gpulda_serve_progress": (C.c_int, [C.c_void_p]),
+    "gpulda_serve_poll": (C.c_int, [C.c_void_p, C.c_uint32, _U64P, _F32P, _F64P, _U32P, _U64P, _U32P]),
+    "gpulda_serve_drain": (C.c_int, [C.c_void_p]),
+    "gpulda_serve_stats": (C.c_int, [C.c_void_p, _U64P, C.c_int]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGNATURES)

@@ -25,6 +25,8 @@ enum Stream : u32 {
   kStreamInitCounts = 1,  // initial n from word counts (src/cu/polyaurn.cu:61-79)
   kStreamPhi = 2,         // x ~ Poisson(beta + n)   (src/cu/polyaurn.cu:87-123)
   kStreamZ = 3,           // topic draws              (src/cu/topics.cu:36-105)
+  kStreamFoldInit = 4,    // fold-in: initial topics of a served document
+  kStreamFold = 5,        // fold-in: topic draws of a served document
 };
 
 // Poisson inversion tables: rows n = 0..kPoisN-1 hold the CDF of

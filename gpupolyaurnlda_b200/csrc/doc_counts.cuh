@@ -1,0 +1,256 @@
+// doc_counts.cuh -- one document's topic counts in shared memory and the
+// per-token topic draw, shared by the Gibbs sweep (zsweep.cu) and the
+// fold-in of new documents against a fixed model (serve.cu).
+//
+// Reference: sample_topics / count_topics / compute_product_cumsum /
+// draw_wary_search / draw_alias, src/cu/topics.cu:36-105 and
+// src/cu/topics.cuh:63-192.  One warp owns one document.  Its counts m_d are
+// a dense array of 16-bit counts plus the sorted list of its nonzero topics
+// and an in-list bitmap.  Per token (after removing its current topic):
+//   B      = sum_k m_dk * q[w][k]      (u64, exact)
+//   sparse iff u0 * (alpha*A[w] + B) < B
+//   sparse: target = floor(u1 * B); topic = first k in ascending order whose
+//           inclusive prefix of m_dk * q[w][k] exceeds target
+//   dense:  slot = floor(u2 * nnz[w]) of the word's alias table; topic = the
+//           slot's own topic if u3 < threshold, else its alias
+//   (alpha*A + B == 0: the topic is kept)
+// then the topic is added back.
+//
+// B and the prefix run over the intersection of the document's topics and the
+// word's nonzero q.  The warp walks whichever list is shorter: the document's
+// sorted topic list (gathering q[w][k]) or the word's list of nonzero q
+// (gathering m_dk from shared memory).  Either way lane l takes the l-th
+// contiguous chunk of an ascending list, so lane order then position is
+// ascending topic order and, the masses being exact integers, both walks
+// select the same topic.
+#pragma once
+
+#include "common.cuh"
+#include "warp.cuh"
+
+namespace gpulda {
+
+// Shared memory per warp for documents of up to Kmax topics: counts and list
+// (2 x Kp u16) and the in-list bitmap.
+__host__ __device__ __forceinline__ size_t doc_counts_bytes(u32 Kmax) {
+  const size_t Kp = (Kmax + 63) & ~63u;
+  return Kp * 4 + ((Kp / 8 + 15) & ~(size_t)15);
+}
+
+struct DocCounts {
+  uint16_t* cnt;  // dense counts, Kp entries
+  // Sorted topics of the document: every topic with a nonzero count, plus
+  // topics whose count fell to zero since the last compaction (their mass is
+  // zero, so they never change B or the selected topic).
+  uint16_t* tl;
+  u32* inl;  // bitmap: topic is in tl
+  u32 nz;    // topics with a nonzero count
+  u32 nl;    // list length (nz plus dead entries)
+};
+
+__device__ __forceinline__ DocCounts doc_counts_at(unsigned char* base, u32 Kmax) {
+  const u32 Kpmax = (Kmax + 63) & ~63u;
+  DocCounts dc;
+  dc.cnt = (uint16_t*)base;
+  dc.tl = dc.cnt + Kpmax;
+  dc.inl = (u32*)(dc.tl + Kpmax);
+  dc.nz = dc.nl = 0;
+  return dc;
+}
+
+// First index i in the sorted list tl[0..n) with tl[i] >= k (warp-cooperative).
+__device__ __forceinline__ u32 list_lower_bound(const uint16_t* tl, u32 n, u32 k, u32 lane) {
+  u32 lo = 0;
+  while (n > 32) {
+    const u32 step = (n + 31) >> 5;
+    const u32 idx = lo + lane * step;
+    const bool lt = lane * step < n && tl[idx] < k;
+    u32 c = __popc(__ballot_sync(kFullMask, lt));
+    if (c == 0) c = 1;
+    lo += (c - 1) * step;
+    n = min(step, n - (c - 1) * step);
+  }
+  const bool lt = lane < n && tl[lo + lane] < k;
+  return lo + __popc(__ballot_sync(kFullMask, lt));
+}
+
+// Drops the entries of topics whose count is zero from the list tl[0..n)
+// (stable, in place, warp-cooperative) and clears their in-list bits.
+// Returns the new length.
+__device__ __forceinline__ u32 list_compact(uint16_t* tl, u32 n, const uint16_t* cnt, u32* inl, u32 lane) {
+  u32 out = 0;
+  for (u32 b = 0; b < n; b += 32) {
+    const u32 e = b + lane;
+    const u32 k = e < n ? tl[e] : 0u;
+    const bool keep = e < n && cnt[k] != 0;
+    const u32 ball = __ballot_sync(kFullMask, keep);
+    __syncwarp();
+    if (keep) tl[out + __popc(ball & ((1u << lane) - 1u))] = (uint16_t)k;
+    if (e < n && !keep) atomicAnd(inl + (k >> 5), ~(1u << (k & 31)));
+    out += __popc(ball);
+    __syncwarp();
+  }
+  return out;
+}
+
+// Inserts k at tl[pos] in a list of n entries (warp-cooperative shift right).
+__device__ __forceinline__ void list_insert(uint16_t* tl, u32 n, u32 pos, u32 k, u32 lane) {
+  for (u32 top = n; top > pos; top = top > pos + 32 ? top - 32 : pos) {
+    const u32 src = top - 1 - lane;
+    const bool act = lane < top - pos && lane < 32;
+    const uint16_t v = act ? tl[src] : 0;
+    __syncwarp();
+    if (act) tl[src + 1] = v;
+    __syncwarp();
+  }
+  if (lane == 0) tl[pos] = (uint16_t)k;
+  __syncwarp();
+}
+
+// Counts and sorted list of the topics z[0..L) of a document with K topics.
+// A topic >= K is counted modulo K and reported in *status.
+__device__ __forceinline__ void doc_counts_build(DocCounts& dc, const u32* z, u32 L, u32 K, u32 lane, u32* status,
+                                                 u32 bad_topic_bit) {
+  const u32 Kp = (K + 63) & ~63u;
+  for (u32 i = lane; i < Kp / 8; i += 32) reinterpret_cast<uint4*>(dc.cnt)[i] = make_uint4(0, 0, 0, 0);
+  for (u32 i = lane; i < Kp / 32; i += 32) dc.inl[i] = 0;
+  __syncwarp();
+  for (u32 i = lane; i < L; i += 32) {
+    u32 k = z[i];
+    if (k >= K) {
+      *status |= bad_topic_bit;
+      k %= K;
+    }
+    atomicAdd(reinterpret_cast<u32*>(dc.cnt) + (k >> 1), 1u << ((k & 1) * 16));
+  }
+  __syncwarp();
+  // lane l compacts its contiguous range of topics
+  const u32 per = Kp / 32;
+  const u32 k0 = lane * per;
+  u32 c = 0;
+  for (u32 k = k0; k < k0 + per; ++k) c += dc.cnt[k] != 0;
+  u32 pos = c;
+#pragma unroll
+  for (u32 o = 1; o < 32; o <<= 1) {
+    const u32 y = __shfl_up_sync(kFullMask, pos, o);
+    if (lane >= o) pos += y;
+  }
+  dc.nz = __shfl_sync(kFullMask, pos, 31);
+  pos -= c;
+  for (u32 k = k0; k < k0 + per; ++k)
+    if (dc.cnt[k]) {
+      dc.tl[pos++] = (uint16_t)k;
+      atomicOr(dc.inl + (k >> 5), 1u << (k & 31));
+    }
+  __syncwarp();
+  dc.nl = dc.nz;
+}
+
+// One token (lane j's in the current chunk): removes topic zj, draws the new
+// topic, adds it back.  r0/r1 are the token's uniform words (already
+// broadcast); my_r3 / my_al are lane j's fourth word and the alias entry of
+// its dense slot (broadcast only when the dense branch runs).  qrow / crow are
+// the word's fixed-point Phi row and nonzero list, nw its list length, Aw its
+// dense mass.  Returns the topic; *nz_minus receives the document's distinct
+// topics without the token, *sparse whether the sparse branch chose it.
+__device__ __forceinline__ u32 token_step(DocCounts& dc, u32 zj, u32 r0, u32 r1, u32 my_r3, u64 my_al, u32 j,
+                                          const u32* __restrict__ qrow, const u64* __restrict__ crow, u32 nw, u64 Aw,
+                                          float alpha, u32 lane, u32* nz_minus, bool* sparse) {
+  uint16_t* cnt = dc.cnt;
+  uint16_t* tl = dc.tl;
+  // remove the token's current topic
+  const u32 cz = cnt[zj];
+  __syncwarp();
+  if (lane == 0) cnt[zj] = (uint16_t)(cz - 1u);
+  if (cz == 1u) --dc.nz;  // the entry stays in the list until compaction
+  __syncwarp();
+  const u32 nl = dc.nl;
+  const bool word_side = nw < nl;
+  // Sparse mass over this lane's contiguous chunk.
+  const u32 len = word_side ? nw : nl;
+  const u32 cper = (len + 31) >> 5;
+  const u32 e0 = min(len, lane * cper), e1 = min(len, e0 + cper);
+  u64 ls = 0;
+  if (word_side) {
+    for (u32 e = e0; e < e1; ++e) {
+      const u64 ent = __ldg(crow + e);
+      ls += (u64)cnt[(u32)ent & 0xffffu] * (u32)(ent >> 32);
+    }
+  } else {
+    for (u32 e = e0; e < e1; ++e) {
+      const u32 k = tl[e];
+      ls += (u64)cnt[k] * __ldg(qrow + k);
+    }
+  }
+  const u64 incl = warp_incl_scan_u64(ls, lane);
+  const u64 B = __shfl_sync(kFullMask, incl, 31);
+  int degenerate;
+  const int sp = take_sparse(r0, alpha, Aw, B, &degenerate);
+  u32 k = zj;
+  if (!degenerate) {
+    if (sp) {
+      const u64 target = scale_u32(r1, B);
+      const u32 f = __ffs(__ballot_sync(kFullMask, incl > target)) - 1;
+      u64 run = __shfl_sync(kFullMask, incl - ls, f);
+      // Finish inside lane f's chunk, 32 candidates at a time.
+      const u32 f0 = min(len, f * cper), f1 = min(len, f0 + cper);
+      for (u32 s0 = f0; s0 < f1; s0 += 32) {
+        const u32 e = s0 + lane;
+        u64 mass = 0;
+        u32 kk = 0;
+        if (e < f1) {
+          if (word_side) {
+            const u64 ent = __ldg(crow + e);
+            kk = (u32)ent & 0xffffu;
+            mass = (u64)cnt[kk] * (u32)(ent >> 32);
+          } else {
+            kk = tl[e];
+            mass = (u64)cnt[kk] * __ldg(qrow + kk);
+          }
+        }
+        const u64 in2 = warp_incl_scan_u64(mass, lane);
+        const u64 tot = __shfl_sync(kFullMask, in2, 31);
+        if (run + tot > target) {
+          const u32 jj = __ffs(__ballot_sync(kFullMask, run + in2 > target)) - 1;
+          k = __shfl_sync(kFullMask, kk, jj);
+          break;
+        }
+        run += tot;
+      }
+    } else {
+      const u32 r3 = __shfl_sync(kFullMask, my_r3, j);
+      const u64 e = __shfl_sync(kFullMask, my_al, j);
+      k = alias_pick(e, r3);
+    }
+  }
+  *sparse = sp && !degenerate;
+  *nz_minus = dc.nz;
+  // add the new topic
+  const u32 ck = cnt[k];
+  __syncwarp();
+  if (lane == 0) cnt[k] = (uint16_t)(ck + 1u);
+  if (ck == 0u) {
+    ++dc.nz;
+    if (!((dc.inl[k >> 5] >> (k & 31)) & 1u)) {
+      list_insert(tl, dc.nl, list_lower_bound(tl, dc.nl, k, lane), k, lane);
+      if (lane == 0) atomicOr(dc.inl + (k >> 5), 1u << (k & 31));
+      __syncwarp();
+      ++dc.nl;
+    }
+  }
+  if (dc.nl - dc.nz > 32u) dc.nl = list_compact(tl, dc.nl, cnt, dc.inl, lane);
+  return k;
+}
+
+// sum over the document's topics of lgamma(alpha + m_dk) - lgamma(alpha)
+// (warp-reduced, every lane receives it).
+__device__ __forceinline__ double doc_lgamma_sum(const DocCounts& dc, float alpha, double lg_a, u32 lane) {
+  double dl = 0.0;
+  for (u32 e = lane; e < dc.nl; e += 32) {
+    const u32 c = dc.cnt[dc.tl[e]];
+    if (c) dl += lgamma((double)alpha + (double)c) - lg_a;
+  }
+  return warp_sum_f64(dl);
+}
+
+}  // namespace gpulda

@@ -503,6 +503,12 @@ int pipelined_sweep(Buffer* b, BufCtx* ctx) {
 
 namespace gpulda {
 int report_error(int code, const char* what) { return fail(code, what); }
+bool current_model(ModelDev* out, int* t) {
+  if (!g.live) return false;
+  *out = g.dev;
+  *t = g.t;
+  return true;
+}
 int report_cuda_error(cudaError_t e, const char* where) { return cuda_fail(e, where); }
 }  // namespace gpulda
 

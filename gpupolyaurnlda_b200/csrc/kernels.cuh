@@ -95,6 +95,9 @@ int device_sm_count();
 // `code` as the last error and, in fatal mode, prints and exits.
 int report_error(int code, const char* what);
 int report_cuda_error(cudaError_t e, const char* where);
+// The single model of gpulda.h, if initialized: its device arrays and the
+// iteration of its last Phi step (-1 before the first).
+bool current_model(ModelDev* out, int* t);
 
 // n[w][k] ~ Poisson(beta + floor(C[w] / K)), iteration 0, stream kStreamInitCounts.
 void launch_init_counts(const ModelDev& m, const u32* C, cudaStream_t s);

@@ -58,6 +58,9 @@ def lib() -> C.CDLL:
         L.orc_sparse_select.restype = C.c_uint32
         L.orc_count_topics.argtypes = [_U32P, C.c_uint32, C.c_uint32, _U32P]
         L.orc_count_topics.restype = C.c_uint32
+        L.orc_fold_in.argtypes = [C.c_uint32, C.c_uint32, C.c_float, _U32P, _U64P, _U64P, _U32P, _U32P, _U32P,
+                                  _U64P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_float),
+                                  _F64P, _U32P, _U32P, C.c_int]
         _lib = L
     return _lib
 
@@ -188,6 +191,25 @@ def z_sweep(K: int, V: int, alpha: float, phi: dict, w: np.ndarray, z: np.ndarra
                       _p32(z), _p32(d_len), len(d_len), tok_base, t, key0, key1, _p32(n_out), _p64(stats),
                       ll.ctypes.data_as(_F64P) if want_ll else None, _p32(K_d), threads or default_threads())
     return {"n": n_out, "stats": stats, "ll": float(ll[0]), "ll_skipped": int(ll[1]), "K_d": K_d}
+
+
+def fold_in(K: int, V: int, alpha: float, phi: dict, w: np.ndarray, lengths: np.ndarray, ids: np.ndarray,
+            n_iter: int, seed: int = 0, chain: int = 0, threads=None) -> dict:
+    """Fold-in of new documents against a fixed model (phi: q, alias, A, nnz
+    of a Phi step): theta (float32, n x K), loglik, skipped, final topics."""
+    w = np.ascontiguousarray(w, np.uint32)
+    lengths = np.ascontiguousarray(lengths, np.uint32)
+    ids = np.ascontiguousarray(ids, np.uint64)
+    n = len(lengths)
+    theta = np.empty(n * K, np.float32)
+    ll = np.empty(n, np.float64)
+    skipped = np.empty(n, np.uint32)
+    z = np.empty(max(1, len(w)), np.uint32)
+    lib().orc_fold_in(K, V, alpha, _p32(phi["q"]), _p64(phi["alias"]), _p64(phi["A"]), _p32(phi["nnz"]), _p32(w),
+                      _p32(lengths), _p64(ids), n, seed & 0xffffffff, chain, n_iter,
+                      theta.ctypes.data_as(C.POINTER(C.c_float)), ll.ctypes.data_as(_F64P), _p32(skipped), _p32(z),
+                      threads or default_threads())
+    return {"theta": theta.reshape(n, K), "ll": ll, "skipped": skipped, "z": z[:len(w)]}
 
 
 class Chain:

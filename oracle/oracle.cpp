@@ -38,7 +38,7 @@ typedef int64_t i64;
 namespace {
 
 constexpr u32 POIS_N = 64, POIS_W = 192, LFAC_N = 256, PTRS_MAX = 64;
-constexpr u32 STREAM_INIT = 1, STREAM_PHI = 2, STREAM_Z = 3;
+constexpr u32 STREAM_INIT = 1, STREAM_PHI = 2, STREAM_Z = 3, STREAM_FOLD_INIT = 4, STREAM_FOLD = 5;
 
 struct W4 {
   u32 v[4];
@@ -406,6 +406,38 @@ void orc_doc_offsets(const u32* d_len, u32 n_docs, u64* d_idx) {
   }
 }
 
+// New topic of a token whose current topic zi has already been removed from
+// the document's counts m (nonzero topics flagged in bits): the mixture of
+// the sparse part sum_k m_k q[k] and the dense part alpha * A (src/cu/
+// topics.cu:36-105, topics.cuh:63-192).  *sparse: the sparse part chose it.
+static u32 draw_topic(u32 K, float alpha, const u32* qrow, const u64* alrow, u64 Aw, u32 nnzw, const u32* m,
+                      const u64* bits, u32 nwords, const W4& r, u32 zi, bool* sparse) {
+  u64 B = 0;
+  for (u32 bw = 0; bw < nwords; ++bw)
+    for (u64 bm = bits[bw]; bm; bm &= bm - 1) {
+      const u32 k = bw * 64 + (u32)__builtin_ctzll(bm);
+      B += (u64)m[k] * qrow[k];
+    }
+  const double tot = (double)alpha * (double)Aw + (double)B;
+  const double u = (double)r.v[0] * (1.0 / 4294967296.0);
+  *sparse = false;
+  if (!(tot > 0.0)) return zi;
+  if (u * tot < (double)B) {
+    *sparse = true;
+    const u64 target = (u64)r.v[1] * (B >> 32) + (((u64)r.v[1] * (B & 0xffffffffULL)) >> 32);
+    u64 run = 0;
+    for (u32 bw = 0; bw < nwords; ++bw)
+      for (u64 bm = bits[bw]; bm; bm &= bm - 1) {
+        const u32 kc = bw * 64 + (u32)__builtin_ctzll(bm);
+        run += (u64)m[kc] * qrow[kc];
+        if (run > target) return kc;
+      }
+    return K;  // unreachable: the prefix reaches B > target
+  }
+  // dense part: the word's sparse alias table has nnzw slots
+  return orc_alias_draw(alrow, nnzw, r.v[2], r.v[3]);
+}
+
 // One z sweep over n_docs documents laid out back to back in w/z.
 // n_out (word-major, V*K) is incremented for every token's new topic.
 // stats[0] += tokens, [1] += docs, [2] += sum min(nnz(m_d^-i), nnz[w]),
@@ -449,36 +481,9 @@ void orc_z_sweep(u32 K, u32 V, float alpha, const u32* q, const u64* al, const u
           --nzd;
         }
         const W4 r = draw(tok_base + off + i, t, STREAM_Z, 0, k0, k1);
-        u64 B = 0;
-        for (u32 bw = 0; bw < nwords; ++bw)
-          for (u64 bm = bits[bw]; bm; bm &= bm - 1) {
-            const u32 k = bw * 64 + (u32)__builtin_ctzll(bm);
-            B += (u64)m[k] * q[row + k];
-          }
-        const double tot = (double)alpha * (double)A[wi] + (double)B;
-        const double u = (double)r.v[0] * (1.0 / 4294967296.0);
-        u32 k;
         bool sparse = false;
-        if (!(tot > 0.0)) {
-          k = zi;
-        } else if (u * tot < (double)B) {
-          sparse = true;
-          const u64 target = (u64)r.v[1] * (B >> 32) + (((u64)r.v[1] * (B & 0xffffffffULL)) >> 32);
-          u64 run = 0;
-          k = K;
-          for (u32 bw = 0; bw < nwords && k == K; ++bw)
-            for (u64 bm = bits[bw]; bm; bm &= bm - 1) {
-              const u32 kc = bw * 64 + (u32)__builtin_ctzll(bm);
-              run += (u64)m[kc] * q[row + kc];
-              if (run > target) {
-                k = kc;
-                break;
-              }
-            }
-        } else {
-          // dense part: the word's sparse alias table has nnz[wi] slots
-          k = orc_alias_draw(al + row, nnz[wi], r.v[2], r.v[3]);
-        }
+        const u32 k = draw_topic(K, alpha, q + row, al + row, A[wi], nnz[wi], m.data(), bits.data(), nwords, r, zi,
+                                 &sparse);
         s_S += std::min<u64>(nzd, nnz[wi]);
         s_sp += sparse ? 1 : 0;
         if (m[k]++ == 0) {
@@ -522,6 +527,68 @@ void orc_z_sweep(u32 K, u32 V, float alpha, const u32* q, const u64* al, const u
       ll[0] += lls[2 * i];
       ll[1] += lls[2 * i + 1];
     }
+}
+
+// Fold-in of new documents against a fixed model (no count rebuild).  For
+// document r (length len[r], id ids[r]): topics start at floor(u * K) with
+// u from Philox (token, id low bits, 0, STREAM_FOLD_INIT) under key (k0,
+// k1 ^ id high bits), then n_iter sweeps draw every token as the z sweep does
+// with counter (token, id low bits, iteration, STREAM_FOLD).  Outputs
+// theta[r][k] = (float)((m_k + alpha) / (L + K alpha)), the log-likelihood
+// sum_i log sum_k theta_k q[w_i][k] / 2^32 over tokens whose word has mass
+// (the others are counted in skipped), and the final topics in z_out.
+void orc_fold_in(u32 K, u32 V, float alpha, const u32* q, const u64* al, const u64* A, const u32* nnz, const u32* w,
+                 const u32* len, const u64* ids, u32 n_docs, u32 k0, u32 k1, u32 n_iter, float* theta, double* ll,
+                 u32* skipped, u32* z_out, int threads) {
+  std::vector<u64> offs(n_docs);
+  orc_doc_offsets(len, n_docs, offs.data());
+  const u32 nwords = (K + 63) / 64;
+  parallel_for(n_docs, std::max(1, threads), [&](u64 a, u64 b, int) {
+    std::vector<u32> m(K);
+    std::vector<u64> bits(nwords);
+    for (u64 d = a; d < b; ++d) {
+      const u32 L = len[d];
+      const u32* wd = w + offs[d];
+      u32* z = z_out + offs[d];
+      const u64 ridx = (u64)(u32)ids[d] << 32;
+      const u32 kk1 = k1 ^ (u32)(ids[d] >> 32);
+      std::fill(m.begin(), m.end(), 0);
+      std::fill(bits.begin(), bits.end(), 0);
+      for (u32 i = 0; i < L; ++i) {
+        const W4 r = draw(ridx | i, 0, STREAM_FOLD_INIT, 0, k0, kk1);
+        z[i] = (u32)(((u64)r.v[0] * K) >> 32);
+        if (m[z[i]]++ == 0) bits[z[i] >> 6] |= 1ull << (z[i] & 63);
+      }
+      for (u32 t = 0; t < n_iter; ++t)
+        for (u32 i = 0; i < L; ++i) {
+          const u32 wi = wd[i] % V, zi = z[i];
+          const u64 row = (u64)wi * K;
+          if (--m[zi] == 0) bits[zi >> 6] &= ~(1ull << (zi & 63));
+          const W4 r = draw(ridx | i, t, STREAM_FOLD, 0, k0, kk1);
+          bool sparse;
+          const u32 k = draw_topic(K, alpha, q + row, al + row, A[wi], nnz[wi], m.data(), bits.data(), nwords, r,
+                                   zi, &sparse);
+          if (m[k]++ == 0) bits[k >> 6] |= 1ull << (k & 63);
+          z[i] = k;
+        }
+      const double denom = (double)L + (double)K * (double)alpha;
+      for (u32 k = 0; k < K; ++k) theta[d * K + k] = (float)(((double)m[k] + (double)alpha) / denom);
+      double s_ll = 0.0;
+      u32 skip = 0;
+      for (u32 i = 0; i < L; ++i) {
+        const u64 row = (u64)(wd[i] % V) * K;
+        double s = 0.0;
+        for (u32 k = 0; k < K; ++k)
+          if (q[row + k]) s += ((double)m[k] + (double)alpha) * (double)q[row + k];
+        if (s > 0.0)
+          s_ll += std::log(s);
+        else
+          ++skip;
+      }
+      ll[d] = s_ll - (double)(L - skip) * (std::log(denom) + 22.18070977791825);
+      skipped[d] = skip;
+    }
+  });
 }
 
 }  // extern "C"
