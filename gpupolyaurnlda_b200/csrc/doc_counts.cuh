@@ -170,8 +170,33 @@ __device__ __forceinline__ u32 token_step(DocCounts& dc, u32 zj, u32 r0, u32 r1,
   const u32 len = word_side ? nw : nl;
   const u32 cper = (len + 31) >> 5;
   const u32 e0 = min(len, lane * cper), e1 = min(len, e0 + cper);
+  // Chunks of at most 4 elements (lists up to 128 entries): unrolled
+  // independent loads, masses kept in registers, so the selection needs no
+  // second pass; the crossing element's topic is read once afterwards.
+  constexpr u32 kRegChunk = 4;
+  const bool in_regs = cper <= kRegChunk;
+  u64 ms[kRegChunk];
   u64 ls = 0;
-  if (word_side) {
+  if (in_regs) {
+    const u32 n_my = e1 - e0;
+    if (word_side) {
+      u64 ent[kRegChunk];
+#pragma unroll
+      for (u32 c = 0; c < kRegChunk; ++c) ent[c] = c < n_my ? __ldg(crow + e0 + c) : 0ull;
+#pragma unroll
+      for (u32 c = 0; c < kRegChunk; ++c) ms[c] = (u64)cnt[(u32)ent[c] & 0xffffu] * (u32)(ent[c] >> 32);
+    } else {
+      u32 ks[kRegChunk], qs[kRegChunk];
+#pragma unroll
+      for (u32 c = 0; c < kRegChunk; ++c) ks[c] = c < n_my ? (u32)tl[e0 + c] : 0u;
+#pragma unroll
+      for (u32 c = 0; c < kRegChunk; ++c) qs[c] = c < n_my ? __ldg(qrow + ks[c]) : 0u;
+#pragma unroll
+      for (u32 c = 0; c < kRegChunk; ++c) ms[c] = (u64)cnt[ks[c]] * qs[c];
+    }
+#pragma unroll
+    for (u32 c = 0; c < kRegChunk; ++c) ls += ms[c];
+  } else if (word_side) {
     for (u32 e = e0; e < e1; ++e) {
       const u64 ent = __ldg(crow + e);
       ls += (u64)cnt[(u32)ent & 0xffffu] * (u32)(ent >> 32);
@@ -191,31 +216,48 @@ __device__ __forceinline__ u32 token_step(DocCounts& dc, u32 zj, u32 r0, u32 r1,
     if (sp) {
       const u64 target = scale_u32(r1, B);
       const u32 f = __ffs(__ballot_sync(kFullMask, incl > target)) - 1;
-      u64 run = __shfl_sync(kFullMask, incl - ls, f);
-      // Finish inside lane f's chunk, 32 candidates at a time.
-      const u32 f0 = min(len, f * cper), f1 = min(len, f0 + cper);
-      for (u32 s0 = f0; s0 < f1; s0 += 32) {
-        const u32 e = s0 + lane;
-        u64 mass = 0;
-        u32 kk = 0;
-        if (e < f1) {
-          if (word_side) {
-            const u64 ent = __ldg(crow + e);
-            kk = (u32)ent & 0xffffu;
-            mass = (u64)cnt[kk] * (u32)(ent >> 32);
-          } else {
-            kk = tl[e];
-            mass = (u64)cnt[kk] * __ldg(qrow + kk);
+      if (in_regs) {
+        // Lane f's first element whose inclusive prefix exceeds the target
+        // (prefixes grow with c, so going down the last hit is the first);
+        // every lane computes its own, lane f's is broadcast.
+        u64 pre = incl - ls;
+        u32 cx = kRegChunk - 1;
+#pragma unroll
+        for (u32 c = kRegChunk - 1; c-- > 0;) {
+          u64 t = pre;
+#pragma unroll
+          for (u32 d = 0; d <= c; ++d) t += ms[d];
+          if (t > target) cx = c;
+        }
+        const u32 ef = f * cper + __shfl_sync(kFullMask, cx, f);
+        k = word_side ? ((u32)__ldg(crow + ef) & 0xffffu) : (u32)tl[ef];
+      } else {
+        u64 run = __shfl_sync(kFullMask, incl - ls, f);
+        // Finish inside lane f's chunk, 32 candidates at a time.
+        const u32 f0 = min(len, f * cper), f1 = min(len, f0 + cper);
+        for (u32 s0 = f0; s0 < f1; s0 += 32) {
+          const u32 e = s0 + lane;
+          u64 mass = 0;
+          u32 kk = 0;
+          if (e < f1) {
+            if (word_side) {
+              const u64 ent = __ldg(crow + e);
+              kk = (u32)ent & 0xffffu;
+              mass = (u64)cnt[kk] * (u32)(ent >> 32);
+            } else {
+              kk = tl[e];
+              mass = (u64)cnt[kk] * __ldg(qrow + kk);
+            }
           }
+          const u64 in2 = warp_incl_scan_u64(mass, lane);
+          const u64 tot = __shfl_sync(kFullMask, in2, 31);
+          if (run + tot > target) {
+            const u32 jj = __ffs(__ballot_sync(kFullMask, run + in2 > target)) - 1;
+            k = __shfl_sync(kFullMask, kk, jj);
+            break;
+          }
+          run += tot;
         }
-        const u64 in2 = warp_incl_scan_u64(mass, lane);
-        const u64 tot = __shfl_sync(kFullMask, in2, 31);
-        if (run + tot > target) {
-          const u32 jj = __ffs(__ballot_sync(kFullMask, run + in2 > target)) - 1;
-          k = __shfl_sync(kFullMask, kk, jj);
-          break;
-        }
-        run += tot;
       }
     } else {
       const u32 r3 = __shfl_sync(kFullMask, my_r3, j);

@@ -19,6 +19,7 @@ namespace {
 
 constexpr u32 kMaxDocLen = 65535u;
 constexpr size_t kZMaxSmem = 200 * 1024;
+constexpr size_t kTokStageBytes = 32 * 32;  // per warp: 32 tokens x 32 bytes
 
 struct ZKernelArgs {
   ModelDev m;
@@ -40,7 +41,9 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
   const ZLaunch& p = a.z;
   const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const u32 V = m.V;
-  DocCounts dc = doc_counts_at(zsm + (size_t)warp * doc_counts_bytes(a.Kmax), a.Kmax);
+  unsigned char* wsm = zsm + (size_t)warp * (doc_counts_bytes(a.Kmax) + kTokStageBytes);
+  DocCounts dc = doc_counts_at(wsm, a.Kmax);
+  uint4* stage = reinterpret_cast<uint4*>(wsm + doc_counts_bytes(a.Kmax));
   const bool want_ll = (p.flags & 1u) && p.ll;
 
   u64 st_tok = 0, st_docs = 0, st_S = 0, st_sp = 0;
@@ -105,13 +108,19 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
       const u64 my_al = (valid && my_nw) ? __ldg(m.al + my_row + my_s) : 0ull;
       u32 new_z = my_z;
       const u32 nt = min(32u, L - base);
+      // The chunk's per-token data is staged in shared memory and read back
+      // with two 16-byte broadcast loads per token instead of eight
+      // shuffles: shuffles and shared loads share the L1 data pipe, which
+      // bounds this kernel.
+      __syncwarp();
+      stage[2 * lane] = make_uint4(my_z, r.x, r.y, my_nw);
+      stage[2 * lane + 1] = make_uint4((u32)my_row, (u32)(my_row >> 32), (u32)my_A, (u32)(my_A >> 32));
+      __syncwarp();
       for (u32 j = 0; j < nt; ++j) {
-        const u32 zj = __shfl_sync(kFullMask, my_z, j);
-        const u32 r0 = __shfl_sync(kFullMask, r.x, j);
-        const u32 r1 = __shfl_sync(kFullMask, r.y, j);
-        const size_t row = (size_t)__shfl_sync(kFullMask, my_row, j);
-        const u32 nw = __shfl_sync(kFullMask, my_nw, j);
-        const u64 Aw = __shfl_sync(kFullMask, my_A, j);
+        const uint4 s0 = stage[2 * j], s1 = stage[2 * j + 1];
+        const u32 zj = s0.x, r0 = s0.y, r1 = s0.z, nw = s0.w;
+        const size_t row = ((u64)s1.y << 32) | s1.x;
+        const u64 Aw = ((u64)s1.w << 32) | s1.z;
         u32 nzm;
         bool sp;
         const u32 k = token_step(dc, zj, r0, r1, r.w, my_al, j, m.q + row, m.csr + row, nw, Aw, alpha, lane, &nzm,
@@ -172,7 +181,7 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
 
 template <bool BATCH>
 void launch_impl(const ZKernelArgs& a, u32 n_docs, cudaStream_t s, u32 wpb, u32 blocks_per_sm) {
-  const size_t per_warp = doc_counts_bytes(a.Kmax);
+  const size_t per_warp = doc_counts_bytes(a.Kmax) + kTokStageBytes;
   // Warps per block: as many as fit the shared-memory budget (at most the request).
   while (wpb > 1 && per_warp * wpb > kZMaxSmem) --wpb;
   const size_t smem = per_warp * wpb;
@@ -192,7 +201,7 @@ void launch_impl(const ZKernelArgs& a, u32 n_docs, cudaStream_t s, u32 wpb, u32 
 
 }  // namespace
 
-size_t z_sweep_smem_per_warp(u32 K) { return doc_counts_bytes(K); }
+size_t z_sweep_smem_per_warp(u32 K) { return doc_counts_bytes(K) + kTokStageBytes; }
 
 void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s) {
   if (!z.n_docs) return;
