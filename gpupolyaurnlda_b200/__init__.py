@@ -123,6 +123,8 @@ _SIGNATURES = {
     "gpulda_set_fatal_errors": (None, [C.c_int]),
     "gpulda_initialize_ex": (C.c_int, [C.POINTER(Args), C.POINTER(Buffer), C.c_uint32, C.POINTER(ExArgs)]),
     "gpulda_set_stream": (C.c_int, [C.c_void_p]),
+    "gpulda_pin_host": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32]),
+    "gpulda_unpin_host": (C.c_int, [C.c_void_p]),
     "gpulda_loglik": (C.c_int, [_F64P, _U64P]),
     "gpulda_corpus_load": (C.c_int, [_U32P, _U32P, _U32P, C.c_uint32, C.c_uint64]),
     "gpulda_corpus_sweep": (C.c_int, [C.c_uint32]),

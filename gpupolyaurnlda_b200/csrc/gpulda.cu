@@ -42,8 +42,12 @@ struct BufCtx {
   cudaStream_t piece[kPieces] = {};  // one stream per piece, so piece sweeps overlap
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // [0] order copied, [1] last copy out issued
   cudaEvent_t in[kPieces] = {}, out[kPieces] = {};
+  cudaEvent_t offs = nullptr;     // document offsets of the current sweep are ready
   bool used = false;
   u32* order = nullptr;           // device: document processing order
+  // Device work counters of this buffer's launches (2 + kPieces), so sweeps
+  // of different buffers may be in flight at the same time.
+  u32* work = nullptr;
   std::vector<u32> order_host;    // host staging of the order
 };
 
@@ -310,6 +314,7 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
     CK(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
     for (auto& ps : ctx->piece) CK(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
     for (auto& e : ctx->ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ctx->offs, cudaEventDisableTiming));
     for (u32 i = 0; i < kPieces; ++i) {
       CK(cudaEventCreateWithFlags(&ctx->in[i], cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&ctx->out[i], cudaEventDisableTiming));
@@ -319,7 +324,7 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
     b.gpu_rng = ctx;
     u32 *z, *w, *dl, *di, *kd;
     if ((rc = dalloc(&z, g.buffer_size)) || (rc = dalloc(&w, g.buffer_size)) || (rc = dalloc(&dl, g.max_D)) ||
-        (rc = dalloc(&di, g.max_D)) || (rc = dalloc(&kd, g.max_D)) || (rc = dalloc(&ctx->order, g.max_D)))
+        (rc = dalloc(&di, g.max_D)) || (rc = dalloc(&kd, g.max_D)) || (rc = dalloc(&ctx->order, g.max_D)) || (rc = dalloc(&ctx->work, 2 + kPieces)))
       return rc;
     b.gpu_z = z;
     b.gpu_w = w;
@@ -387,8 +392,9 @@ int z_launch(cudaStream_t s, u32* z, const u32* w, const u32* d_len, const u32* 
 }
 
 // With a split (large K), `order` lists the short documents first.
+// `work` holds 2 + kPieces zeroed-per-launch counters.
 int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_idx, const u32* order, u32* K_d,
-                 u32 n_docs, u64 n_tokens, bool offsets, cudaEvent_t* ev, const DocSplit* split = nullptr) {
+                 u32 n_docs, u64 n_tokens, bool offsets, cudaEvent_t* ev, u32* work, const DocSplit* split = nullptr) {
   CK(cudaEventRecord(ev[0], s));
   if (offsets) {
     launch_doc_offsets(d_len, d_idx, n_docs, s);
@@ -403,14 +409,14 @@ int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_
     CK(cudaStreamWaitEvent(g.side, g.fork, 0));
     if (n_docs > split->n_short)
       rc = z_launch(s, z, w, d_len, d_idx, order + split->n_short, K_d, n_docs - split->n_short, n_tokens,
-                    g.tok_offset, g.work, split->lmax_long);
+                    g.tok_offset, work, split->lmax_long);
     if (!rc && split->n_short)
       rc = z_launch(g.side, z, w, d_len, d_idx, order, K_d, split->n_short, n_tokens, g.tok_offset,
-                    g.work + 1 + kPieces, kShortDoc);
+                    work + 1 + kPieces, kShortDoc);
     CK(cudaEventRecord(g.join, g.side));
     CK(cudaStreamWaitEvent(s, g.join, 0));
   } else {
-    rc = z_launch(s, z, w, d_len, d_idx, order, K_d, n_docs, n_tokens, g.tok_offset, g.work);
+    rc = z_launch(s, z, w, d_len, d_idx, order, K_d, n_docs, n_tokens, g.tok_offset, work);
   }
   if (rc) return rc;
   CK(cudaEventRecord(ev[2], s));
@@ -467,6 +473,7 @@ int pipelined_sweep(Buffer* b, BufCtx* ctx) {
   CK(cudaGetLastError());
   g.launches += 1;
   CK(cudaEventRecord(g.z_ev[1], s));
+  CK(cudaEventRecord(ctx->offs, s));
   if (ctx->used) CK(cudaStreamWaitEvent(ctx->h2d, ctx->ev[1], 0));  // the previous copy out has read gpu_z
   const u64 tok_base = g.tok_offset;
   for (u32 p = 0; p < kPieces; ++p) {
@@ -478,11 +485,11 @@ int pipelined_sweep(Buffer* b, BufCtx* ctx) {
     CK(cudaEventRecord(ctx->in[p], ctx->h2d));
     cudaStream_t ps = ctx->piece[p];
     CK(cudaStreamWaitEvent(ps, ctx->in[p], 0));
-    CK(cudaStreamWaitEvent(ps, g.z_ev[1], 0));  // document offsets are ready
+    CK(cudaStreamWaitEvent(ps, ctx->offs, 0));  // document offsets are ready
     const u32 nd = dcut[p + 1] - dcut[p];
     if (nd) {
       const int rc = z_launch(ps, gz, gw, gdl + dcut[p], gdi + dcut[p], ctx->order + dcut[p], gkd + dcut[p], nd,
-                              b->n_tokens, tok_base, g.work + 1 + p);
+                              b->n_tokens, tok_base, ctx->work + 1 + p);
       if (rc) return rc;
     }
     CK(cudaEventRecord(ctx->out[p], ps));
@@ -577,7 +584,7 @@ extern "C" void sample_z_async(Buffer* b) {
   CKV(cudaMemcpyAsync(ctx->order, ctx->order_host.data(), db, cudaMemcpyHostToDevice, s));
   CKV(cudaEventRecord(ctx->ev[0], s));
   if (z_step_async(s, (u32*)b->gpu_z, (const u32*)b->gpu_w, (const u32*)b->gpu_d_len, (u32*)b->gpu_d_idx,
-                   ctx->order, (u32*)b->gpu_K_d, b->n_docs, b->n_tokens, true, g.z_ev, &split))
+                   ctx->order, (u32*)b->gpu_K_d, b->n_docs, b->n_tokens, true, g.z_ev, ctx->work, &split))
     return;
   g.z_timed = true;
   CKV(cudaMemcpyAsync(b->z, b->gpu_z, tb, cudaMemcpyDeviceToHost, s));
@@ -618,6 +625,8 @@ extern "C" void cleanup(Buffer* buffers, uint32_t n_buffers) {
       BufCtx* ctx = (BufCtx*)b.gpu_rng;
       for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+      if (ctx->offs) cudaEventDestroy(ctx->offs);
+      dfree(ctx->work);
       for (u32 k = 0; k < kPieces; ++k) {
         if (ctx->in[k]) cudaEventDestroy(ctx->in[k]);
         if (ctx->out[k]) cudaEventDestroy(ctx->out[k]);
@@ -658,6 +667,27 @@ extern "C" int gpulda_initialize_ex(const Args* args, Buffer* buffers, uint32_t 
   const int rc = init_impl(args, buffers, n_buffers, ex);
   g.fatal = fatal;
   return rc;
+}
+
+extern "C" int gpulda_pin_host(void* p, uint64_t bytes, uint32_t flags) {
+  if (!p || !bytes) return fail(GPULDA_ERR_ARGS, "gpulda_pin_host: empty range");
+  unsigned f = cudaHostRegisterPortable;
+  if (flags & GPULDA_PIN_READ_ONLY) f |= cudaHostRegisterReadOnly;
+  const cudaError_t e = cudaHostRegister(p, (size_t)bytes, f);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // not sticky: the range stays usable unpinned
+    return cuda_fail(e, "cudaHostRegister");
+  }
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_unpin_host(void* p) {
+  const cudaError_t e = cudaHostUnregister(p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return cuda_fail(e, "cudaHostUnregister");
+  }
+  return GPULDA_OK;
 }
 
 extern "C" int gpulda_set_stream(void* s) {
@@ -713,7 +743,7 @@ extern "C" int gpulda_corpus_sweep(uint32_t n_iter) {
   for (u32 i = 0; i < n_iter; ++i) {
     int rc = phi_step_async(s);
     if (rc) return rc;
-    rc = z_step_async(s, g.cz, g.cw, g.cd_len, g.cd_idx, g.corder, g.cK_d, g.c_docs, g.c_tokens, false, g.z_ev,
+    rc = z_step_async(s, g.cz, g.cw, g.cd_len, g.cd_idx, g.corder, g.cK_d, g.c_docs, g.c_tokens, false, g.z_ev, g.work,
                       &g.c_split);
     if (rc) return rc;
     g.z_timed = true;

@@ -89,6 +89,12 @@ void sample_phi(void);
  * completes. */
 void sample_z_async(Buffer* buffer);
 
+/* Buffers are independent on the device (own arrays, streams and work
+ * counters): a host may keep several in flight, calling sample_z_async on the
+ * next buffer before sync_buffer on the previous one (token numbering follows
+ * the order of the sample_z_async calls).  Every buffer must be synced before
+ * the next sample_phi. */
+
 /* Replaces sync_buffer() (src/cu/train.cu:174-177): waits for the buffer. */
 void sync_buffer(Buffer* buffer);
 
@@ -164,6 +170,15 @@ int gpulda_kernel_times(float* ms, int n);
  * nnz(x[.][w])), [3] tokens that took the sparse branch,
  * [4] kernels launched by the library in that iteration. */
 int gpulda_counters(uint64_t* out, int n);
+
+/* Page-locks (pins) a host range so the copies of sample_z_async / sync_buffer
+ * from and to it run as asynchronous DMA; e.g. the memory-mapped z/w/d/K_d
+ * files of a streaming host loop.  GPULDA_PIN_READ_ONLY for ranges mapped
+ * read-only.  Unpin before unmapping.  Returns GPULDA_ERR_CUDA if the range
+ * cannot be pinned (the copies then still work, staged by the driver). */
+#define GPULDA_PIN_READ_ONLY 1u
+int gpulda_pin_host(void* p, uint64_t bytes, uint32_t flags);
+int gpulda_unpin_host(void* p);
 
 /* ---- read-back hooks for the parity tests ------------------------------ */
 
