@@ -27,6 +27,7 @@ GPULDA_ERR_NOMEM = 5
 GPULDA_ERR_DEVICE = 6
 GPULDA_ERR_UNSUPPORTED = 7
 GPULDA_FLAG_LOGLIK = 1
+GPULDA_FLAG_HASHMAP = 2
 GPULDA_MAX_K = 32768
 GPULDA_MAX_DOC_LEN = 65535
 POIS_TABLE_N, POIS_TABLE_W, LOGFAC_N = 64, 192, 256

@@ -385,7 +385,11 @@ int z_launch(cudaStream_t s, u32* z, const u32* w, const u32* d_len, const u32* 
   zl.ll = g.ll;
   zl.work = work;
   zl.status = g.status;
-  if (!(g.K > kMapMinK && lmax && launch_z_sweep_map(g.dev, zl, s, lmax))) launch_z_sweep(g.dev, zl, s);
+  bool done = false;
+  if (g.K > kMapMinK && lmax)
+    done = (g.flags & GPULDA_FLAG_HASHMAP) ? launch_z_sweep_map(g.dev, zl, s, lmax)
+                                           : launch_z_sweep_pairs(g.dev, zl, s, lmax);
+  if (!done) launch_z_sweep(g.dev, zl, s);
   CK(cudaGetLastError());
   g.launches += 1;
   return GPULDA_OK;

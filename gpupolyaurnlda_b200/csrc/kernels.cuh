@@ -129,6 +129,10 @@ size_t z_sweep_smem_per_warp(u32 K);
 // false without launching when lmax needs more shared memory than a block has.
 bool launch_z_sweep_map(const ModelDev& m, const ZLaunch& z, cudaStream_t s, u32 lmax);
 u32 z_map_slots(u32 K, u32 lmax);
+// The same sweep with each document's counts as a sorted list of (topic,
+// count) pairs in shared memory (large K; the default there).
+bool launch_z_sweep_pairs(const ModelDev& m, const ZLaunch& z, cudaStream_t s, u32 lmax);
+u32 z_pairs_cap(u32 K, u32 lmax);
 
 // Debug hooks.
 void launch_debug_philox(const u32* ctr, u32 n, u32 k0, u32 k1, u32* out, cudaStream_t s);

@@ -1,0 +1,396 @@
+// zsweep_pairs.cu -- the z sweep for large K with each document's topic counts
+// as a sorted list of (topic, count) pairs in shared memory (reference: the
+// per-document HashMap of src/cu/hashmap.cuh:13-334 used by sample_topics,
+// src/cu/topics.cu:36-105).
+//
+// The list is the order-preserving map of zsweep_map.cu without empty slots:
+// entries (topic << 16 | count), ascending topic.  A topic whose count falls
+// to zero stays as a dead entry (zero mass, so it never changes B or the
+// selected topic) and is revived if the topic returns; more than 32 dead
+// entries are compacted away.  Lookups are warp-cooperative 32-ary searches
+// (two ballot rounds for lists up to 1024 entries); inserts shift the tail.
+// The walk reads the entries in ascending topic order, so the sparse draw is
+// identical to the dense-count kernel's, the map kernel's and the CPU
+// oracle's.
+//
+// Per token the warp walks the shorter of (i) the document's entries,
+// gathering q[w][k] (counts come with the entries), or (ii) the word's list of
+// nonzero q, each lane finding its topics' counts by binary search in the
+// document's entries.  Lane l takes the l-th contiguous chunk of the walked
+// list; chunks of at most 4 elements keep their masses in registers, so the
+// sparse selection needs no second pass.
+//
+// Capacity per warp: min(lmax, K) live entries, at most 33 dead ones before a
+// compaction, rounded up: min(lmax, K) + 64.  An insert that would pass it is
+// refused and reported (it cannot happen under that bound).
+#include <algorithm>
+#include <cmath>
+
+#include "kernels.cuh"
+#include "warp.cuh"
+
+namespace gpulda {
+
+namespace {
+
+constexpr u32 kMaxDocLen = 65535u;
+constexpr size_t kTokStageBytes = 32 * 32;  // per warp: 32 tokens x 32 bytes
+constexpr u32 kStatusListFull = 32;         // an insert found the list full (cannot happen)
+
+struct PairArgs {
+  ModelDev m;
+  ZLaunch z;
+  u32 cap;       // entries per warp
+  u32 lmax;      // longest document this launch accepts
+  double lg_Ka;  // lgamma(K * alpha)
+  double lg_a;   // lgamma(alpha)
+};
+
+__device__ __forceinline__ u32 topic_of(u32 e) { return e >> 16; }
+__device__ __forceinline__ u32 count_of(u32 e) { return e & 0xffffu; }
+
+// First index i in P[0..n) with topic(P[i]) >= k (warp-cooperative).
+__device__ __forceinline__ u32 pairs_lower_bound(const u32* P, u32 n, u32 k, u32 lane) {
+  u32 lo = 0;
+  while (n > 32) {
+    const u32 step = (n + 31) >> 5;
+    const bool lt = lane * step < n && topic_of(P[lo + lane * step]) < k;
+    u32 c = __popc(__ballot_sync(kFullMask, lt));
+    if (c == 0) c = 1;
+    lo += (c - 1) * step;
+    n = min(step, n - (c - 1) * step);
+  }
+  const bool lt = lane < n && topic_of(P[lo + lane]) < k;
+  return lo + __popc(__ballot_sync(kFullMask, lt));
+}
+
+// Count of topic k in P[0..n) by one lane's binary search.
+__device__ __forceinline__ u32 pairs_count(const u32* P, u32 n, u32 k) {
+  u32 lo = 0, hi = n;
+  while (lo < hi) {
+    const u32 mid = (lo + hi) >> 1;
+    if (topic_of(P[mid]) < k)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return (lo < n && topic_of(P[lo]) == k) ? count_of(P[lo]) : 0u;
+}
+
+// Inserts e at P[pos] in a list of n entries (warp-cooperative shift right).
+__device__ __forceinline__ void pairs_insert(u32* P, u32 n, u32 pos, u32 e, u32 lane) {
+  for (u32 top = n; top > pos; top = top > pos + 32 ? top - 32 : pos) {
+    const u32 src = top - 1 - lane;
+    const bool act = lane < top - pos;
+    const u32 v = act ? P[src] : 0u;
+    __syncwarp();
+    if (act) P[src + 1] = v;
+    __syncwarp();
+  }
+  if (lane == 0) P[pos] = e;
+  __syncwarp();
+}
+
+// Drops dead entries (stable, in place); returns the new length.
+__device__ __forceinline__ u32 pairs_compact(u32* P, u32 n, u32 lane) {
+  u32 out = 0;
+  for (u32 b = 0; b < n; b += 32) {
+    const u32 i = b + lane;
+    const u32 e = i < n ? P[i] : 0u;
+    const bool keep = i < n && count_of(e) != 0;
+    const u32 ball = __ballot_sync(kFullMask, keep);
+    __syncwarp();
+    if (keep) P[out + __popc(ball & ((1u << lane) - 1u))] = e;
+    out += __popc(ball);
+    __syncwarp();
+  }
+  return out;
+}
+
+// Count of topic k += 1 at its position; inserts it if absent.
+__device__ __forceinline__ void pairs_add_at(u32* P, u32& nl, u32& nz, u32 pos, u32 k, u32 cap, u32 lane,
+                                             u32* status) {
+  const u32 e = pos < nl ? P[pos] : 0xffffffffu;
+  __syncwarp();
+  if (pos < nl && topic_of(e) == k) {
+    if (lane == 0) P[pos] = e + 1u;
+    if (count_of(e) == 0) ++nz;  // a dead entry revived
+    __syncwarp();
+    return;
+  }
+  if (nl >= cap) {
+    *status |= kStatusListFull;
+    return;
+  }
+  pairs_insert(P, nl, pos, (k << 16) | 1u, lane);
+  ++nl;
+  ++nz;
+}
+
+__global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
+  extern __shared__ __align__(16) unsigned char zsm[];
+  const ModelDev& m = a.m;
+  const ZLaunch& p = a.z;
+  const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const u32 K = m.K, V = m.V;
+  unsigned char* wsm = zsm + (size_t)warp * ((size_t)a.cap * 4 + kTokStageBytes);
+  u32* P = (u32*)wsm;
+  uint4* stage = (uint4*)(wsm + (size_t)a.cap * 4);
+  const bool want_ll = (p.flags & 1u) && p.ll;
+
+  u64 st_tok = 0, st_docs = 0, st_S = 0, st_sp = 0;
+  double ll_acc = 0.0, ll_skip = 0.0;
+  u32 status = 0;
+
+  while (true) {
+    u32 doc = 0;
+    if (lane == 0) doc = atomicAdd(p.work, 1u);
+    doc = __shfl_sync(kFullMask, doc, 0);
+    if (doc >= p.n_docs) break;
+    if (p.order) doc = p.order[doc];
+    const u32 L = p.d_len[doc];
+    const u64 off = p.d_idx[doc];
+    if (L > kMaxDocLen || L > a.lmax) {
+      status |= kStatusDocTooLong;
+      continue;
+    }
+    if (off + L > p.n_tokens) {
+      status |= kStatusDocRange;
+      continue;
+    }
+    // build the sorted entries of the document's topics
+    u32 nl = 0, nz = 0;
+    for (u32 i = 0; i < L; ++i) {
+      u32 k = p.z[off + i];
+      if (k >= K) {
+        status |= kStatusBadTopic;
+        k %= K;
+      }
+      pairs_add_at(P, nl, nz, pairs_lower_bound(P, nl, k, lane), k, a.cap, lane, &status);
+    }
+
+    for (u32 base = 0; base < L; base += 32) {
+      const u32 i = base + lane;
+      const bool valid = i < L;
+      u32 my_w = valid ? p.w[off + i] : 0;
+      u32 my_z = valid ? p.z[off + i] : 0;
+      if (my_w >= V) {
+        status |= kStatusBadWord;
+        my_w %= V;
+      }
+      if (my_z >= K) my_z %= K;
+      const U4 r = draw4(p.tok_base + off + i, p.t, kStreamZ, 0, m.key0, m.key1);
+      const u32 my_nw = valid ? __ldg(m.nnz + my_w) : 0u;
+      const u64 my_A = valid ? __ldg(m.A + my_w) : 0ull;
+      const u32 my_s = (u32)(((u64)r.z * my_nw) >> 32);
+      const u64 my_row = (u64)my_w * K;
+      const u64 my_al = (valid && my_nw) ? __ldg(m.al + my_row + my_s) : 0ull;
+      u32 new_z = my_z;
+      const u32 nt = min(32u, L - base);
+      __syncwarp();
+      stage[2 * lane] = make_uint4(my_z, r.x, r.y, my_nw);
+      stage[2 * lane + 1] = make_uint4((u32)my_row, (u32)(my_row >> 32), (u32)my_A, (u32)(my_A >> 32));
+      __syncwarp();
+      for (u32 j = 0; j < nt; ++j) {
+        const uint4 s0 = stage[2 * j], s1 = stage[2 * j + 1];
+        const u32 zj = s0.x, r0 = s0.y, r1 = s0.z, nw = s0.w;
+        const size_t row = ((u64)s1.y << 32) | s1.x;
+        const u64 Aw = ((u64)s1.w << 32) | s1.z;
+        const u32* __restrict__ qrow = m.q + row;
+        const u64* __restrict__ crow = m.csr + row;
+        // remove the token's current topic (present with a positive count)
+        {
+          const u32 pz = pairs_lower_bound(P, nl, zj, lane);
+          const u32 e = pz < nl ? P[pz] : 0u;
+          __syncwarp();
+          if (pz < nl && topic_of(e) == zj && count_of(e) > 0) {
+            if (lane == 0) P[pz] = e - 1u;
+            if (count_of(e) == 1) --nz;
+          }
+          __syncwarp();
+        }
+        const bool word_side = nw < nl;
+        const u32 len = word_side ? nw : nl;
+        const u32 cper = (len + 31) >> 5;
+        const u32 e0 = min(len, lane * cper), e1 = min(len, e0 + cper);
+        constexpr u32 kRegChunk = 4;
+        const bool in_regs = cper <= kRegChunk;
+        u64 ms[kRegChunk];
+        u64 ls = 0;
+        if (in_regs) {
+          const u32 n_my = e1 - e0;
+          if (word_side) {
+#pragma unroll
+            for (u32 c = 0; c < kRegChunk; ++c) {
+              const u64 ent = c < n_my ? __ldg(crow + e0 + c) : 0ull;
+              ms[c] = c < n_my ? (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32) : 0ull;
+            }
+          } else {
+            u32 es[kRegChunk], qs[kRegChunk];
+#pragma unroll
+            for (u32 c = 0; c < kRegChunk; ++c) es[c] = c < n_my ? P[e0 + c] : 0u;
+#pragma unroll
+            for (u32 c = 0; c < kRegChunk; ++c) qs[c] = c < n_my ? __ldg(qrow + topic_of(es[c])) : 0u;
+#pragma unroll
+            for (u32 c = 0; c < kRegChunk; ++c) ms[c] = (u64)count_of(es[c]) * qs[c];
+          }
+#pragma unroll
+          for (u32 c = 0; c < kRegChunk; ++c) ls += ms[c];
+        } else if (word_side) {
+          for (u32 e = e0; e < e1; ++e) {
+            const u64 ent = __ldg(crow + e);
+            ls += (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32);
+          }
+        } else {
+          for (u32 e = e0; e < e1; ++e) {
+            const u32 en = P[e];
+            ls += (u64)count_of(en) * __ldg(qrow + topic_of(en));
+          }
+        }
+        const u64 incl = warp_incl_scan_u64(ls, lane);
+        const u64 B = __shfl_sync(kFullMask, incl, 31);
+        int degenerate;
+        const int sp = take_sparse(r0, m.alpha, Aw, B, &degenerate);
+        u32 k = zj;
+        u32 pos = 0xffffffffu;  // the new topic's entry, when the walk found it
+        if (!degenerate) {
+          if (sp) {
+            const u64 target = scale_u32(r1, B);
+            const u32 f = __ffs(__ballot_sync(kFullMask, incl > target)) - 1;
+            u32 ef;
+            if (in_regs) {
+              // lane f's first element whose inclusive prefix exceeds the target
+              u64 pre = incl - ls;
+              u32 cx = kRegChunk - 1;
+#pragma unroll
+              for (u32 c = kRegChunk - 1; c-- > 0;) {
+                u64 t = pre;
+#pragma unroll
+                for (u32 d = 0; d <= c; ++d) t += ms[d];
+                if (t > target) cx = c;
+              }
+              ef = f * cper + __shfl_sync(kFullMask, cx, f);
+            } else {
+              u64 run = __shfl_sync(kFullMask, incl - ls, f);
+              const u32 f0 = min(len, f * cper), f1 = min(len, f0 + cper);
+              ef = f1 - 1;
+              for (u32 s0 = f0; s0 < f1; s0 += 32) {
+                const u32 e = s0 + lane;
+                u64 mass = 0;
+                if (e < f1) {
+                  if (word_side) {
+                    const u64 ent = __ldg(crow + e);
+                    mass = (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32);
+                  } else {
+                    const u32 en = P[e];
+                    mass = (u64)count_of(en) * __ldg(qrow + topic_of(en));
+                  }
+                }
+                const u64 in2 = warp_incl_scan_u64(mass, lane);
+                const u64 tot = __shfl_sync(kFullMask, in2, 31);
+                if (run + tot > target) {
+                  ef = s0 + __ffs(__ballot_sync(kFullMask, run + in2 > target)) - 1;
+                  break;
+                }
+                run += tot;
+              }
+            }
+            if (word_side) {
+              k = (u32)__ldg(crow + ef) & 0xffffu;
+            } else {
+              k = topic_of(P[ef]);
+              pos = ef;
+            }
+          } else {
+            const u32 r3 = __shfl_sync(kFullMask, r.w, j);
+            const u64 e = __shfl_sync(kFullMask, my_al, j);
+            k = alias_pick(e, r3);
+          }
+        }
+        const u32 nzm = nz;
+        if (pos == 0xffffffffu) pos = pairs_lower_bound(P, nl, k, lane);
+        pairs_add_at(P, nl, nz, pos, k, a.cap, lane, &status);
+        if (nl - nz > 32u) nl = pairs_compact(P, nl, lane);
+        if (lane == 0) {
+          atomicAdd(m.n + row + k, 1u);
+          st_S += min(nzm, nw);
+          st_sp += (sp && !degenerate) ? 1 : 0;
+        }
+        if (lane == j) new_z = k;
+        __syncwarp();
+      }
+      if (valid) {
+        p.z[off + i] = new_z;
+        if (want_ll) {  // log Phi[new topic][word], one token per lane
+          const u32 qk = __ldg(m.q + my_row + new_z);
+          if (qk)
+            ll_acc += log((double)qk) - 22.18070977791825;  // 32 log 2
+          else
+            ll_skip += 1.0;
+        }
+      }
+    }
+    if (lane == 0 && p.K_d) p.K_d[doc] = nz;
+    if (want_ll) {
+      double dl = 0.0;
+      for (u32 e = lane; e < nl; e += 32) {
+        const u32 c = count_of(P[e]);
+        if (c) dl += lgamma((double)m.alpha + (double)c) - a.lg_a;
+      }
+      dl = warp_sum_f64(dl);
+      if (lane == 0) ll_acc += dl + a.lg_Ka - lgamma((double)K * (double)m.alpha + (double)L);
+    }
+    st_tok += L;
+    st_docs += 1;
+    __syncwarp();
+  }
+  if (want_ll) {
+    ll_acc = warp_sum_f64(ll_acc);
+    ll_skip = warp_sum_f64(ll_skip);
+  }
+  if (lane == 0) {
+    atomicAdd(p.counters + kCtrTokens, (unsigned long long)st_tok);
+    atomicAdd(p.counters + kCtrDocs, (unsigned long long)st_docs);
+    atomicAdd(p.counters + kCtrSparseWork, (unsigned long long)st_S);
+    atomicAdd(p.counters + kCtrSparseDraws, (unsigned long long)st_sp);
+    if (want_ll) {
+      atomicAdd(p.ll, ll_acc);
+      atomicAdd(p.ll + 1, ll_skip);
+    }
+  }
+  status = __reduce_or_sync(kFullMask, status);
+  if (lane == 0 && status) atomicOr(p.status, status);
+}
+
+}  // namespace
+
+u32 z_pairs_cap(u32 K, u32 lmax) { return ((std::min(std::max(lmax, 1u), K) + 64 + 31) / 32) * 32; }
+
+bool launch_z_sweep_pairs(const ModelDev& m, const ZLaunch& z, cudaStream_t s, u32 lmax) {
+  if (!z.n_docs) return true;
+  PairArgs a;
+  a.m = m;
+  a.z = z;
+  a.lmax = lmax;
+  a.cap = z_pairs_cap(m.K, lmax);
+  a.lg_a = std::lgamma((double)m.alpha);
+  a.lg_Ka = std::lgamma((double)m.K * (double)m.alpha);
+  const size_t per_warp = (size_t)a.cap * 4 + kTokStageBytes;
+  constexpr size_t kBudget = 200 * 1024;
+  u32 wpb = 8;
+  while (wpb > 1 && per_warp * wpb > kBudget) --wpb;
+  if (per_warp * wpb > kBudget) return false;
+  const size_t smem = per_warp * wpb;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(z_sweep_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBudget);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, z_sweep_pairs_kernel, 32 * wpb, smem);
+  if (per_sm < 1) per_sm = 1;
+  u32 blocks = (u32)(device_sm_count() * per_sm);
+  const u32 need = (z.n_docs + wpb - 1) / wpb;
+  if (blocks > need) blocks = need;
+  z_sweep_pairs_kernel<<<blocks, 32 * wpb, smem, s>>>(a);
+  return true;
+}
+
+}  // namespace gpulda

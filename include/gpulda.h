@@ -132,6 +132,9 @@ typedef struct GpuldaExArgs {
 } GpuldaExArgs;
 
 #define GPULDA_FLAG_LOGLIK 1u  /* accumulate the joint log-likelihood per sweep */
+/* K > 2048: keep each document's counts in the order-preserving Robin Hood
+ * hash map instead of the default sorted (topic, count) list (same results). */
+#define GPULDA_FLAG_HASHMAP 2u
 
 /* initialize() with an explicit seed, chain id and flags. Returns an error
  * code (never exits). */

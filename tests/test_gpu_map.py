@@ -1,8 +1,10 @@
-"""GPU parity of the large-K sweep, whose per-document topic counts live in a
-shared-memory Robin Hood hash map (src/cu/hashmap.cuh's role), against the
-CPU oracle: topics and counts bit for bit, through the resident-corpus and the
-buffer entry points, for short documents (one launch) and long ones (a second
-launch sized for the longest)."""
+"""GPU parity of the large-K sweep against the CPU oracle, with each
+document's topic counts in shared memory either as a sorted (topic, count)
+list (the default) or in the order-preserving Robin Hood hash map
+(GPULDA_FLAG_HASHMAP) -- src/cu/hashmap.cuh's role: topics and counts bit for
+bit, through the resident-corpus and the buffer entry points, for short
+documents (one launch) and long ones (a second launch sized for the
+longest)."""
 import dataclasses
 
 import numpy as np
@@ -18,14 +20,18 @@ def _workload(K, V, D, lens=("lognormal", 4.2, 0.6, 5, 2000)):
     return dataclasses.replace(corpus.WORKLOADS["large_k10000"], K=K, V=V, D=D, doc_len=lens)
 
 
+STORES = [0, g.GPULDA_FLAG_HASHMAP]
+
+
+@pytest.mark.parametrize("store", STORES, ids=["pairs", "hashmap"])
 @pytest.mark.parametrize("K,V,D", [(4096, 3000, 3000), (10000, 2000, 1500)])
-def test_map_sweep_matches_oracle(gpu_lib, oracle_lib, K, V, D):
+def test_map_sweep_matches_oracle(gpu_lib, oracle_lib, K, V, D, store):
     c = corpus.generate(_workload(K, V, D), seed=5, device="cuda")
     assert c.d_len.max() > 256 and c.d_len.min() <= 256  # both launches run
     ch = oracle_lib.Chain(c.K, c.alpha, c.beta, c.counts, seed=3)
     z_orc = c.z.copy()
     with g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=3,
-                   flags=g.GPULDA_FLAG_LOGLIK) as s:
+                   flags=g.GPULDA_FLAG_LOGLIK | store) as s:
         s.corpus_load(c.z.copy(), c.w, c.d_len)
         for it in range(3):
             s.corpus_sweep(1)
@@ -40,7 +46,7 @@ def test_map_sweep_matches_oracle(gpu_lib, oracle_lib, K, V, D):
     # the buffer entry point gives the same chain
     z_buf = c.z.copy()
     from gpupolyaurnlda_b200.train import iterate_buffers
-    with g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=200000, max_D=700, seed=3) as s:
+    with g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=200000, max_D=700, seed=3, flags=store) as s:
         for _ in range(3):
             s.sample_phi()
             for zb, wb, db, kb in iterate_buffers(z_buf, c.w, c.d_len, c.k_d(), 200000, 700):
@@ -48,7 +54,8 @@ def test_map_sweep_matches_oracle(gpu_lib, oracle_lib, K, V, D):
     assert (z_buf == z_orc).all()
 
 
-def test_map_clustered_topics(gpu_lib, oracle_lib):
+@pytest.mark.parametrize("store", STORES, ids=["pairs", "hashmap"])
+def test_map_clustered_topics(gpu_lib, oracle_lib, store):
     """Documents whose topics are all distinct and packed at the top of the
     topic range: every insertion lands in one long run near the end of the
     table, the case the tail capacity is sized for."""
@@ -62,7 +69,7 @@ def test_map_clustered_topics(gpu_lib, oracle_lib):
     order = np.argsort(-counts.astype(np.int64), kind="stable")
     counts = counts[order]
     z_gpu = z.copy()
-    with g.Sampler(0.01, 0.05, K, counts, buffer_size=16, max_D=4, seed=1) as s:
+    with g.Sampler(0.01, 0.05, K, counts, buffer_size=16, max_D=4, seed=1, flags=store) as s:
         s.corpus_load(z_gpu, w, lens)
         n0 = s.read_state(q=False, alias=False, A=False, S=False, nnz=False)["n"]
         s.corpus_sweep(1)
