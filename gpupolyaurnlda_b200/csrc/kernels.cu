@@ -150,14 +150,13 @@ __global__ void __launch_bounds__(256) phi_draw_batch_kernel(ModelDev ar, BatchP
 // wq[n] holds the weights, key[n] the items' topics; vals[n], idx[n] scratch.
 // Block-cooperative.
 // ---------------------------------------------------------------------------
-__device__ void alias_build_block(const u64* wq, const uint16_t* key, u32 n, u64 A, u64* vals, uint16_t* idx,
-                                  u64* out, u64* sh) {
+__device__ void alias_build_block(const u64* ent, u32 n, u64 A, u64* vals, uint16_t* idx, u64* out, u64* sh) {
   const u32 NT = blockDim.x, tid = threadIdx.x;
   const u32 chunk = (n + NT - 1) / NT;
   const u32 i0 = min(n, tid * chunk), i1 = min(n, i0 + chunk);
   u64 nl = 0, dl = 0, nh = 0, eh = 0;
   for (u32 i = i0; i < i1; ++i) {
-    const u64 wi = (u64)n * wq[i];
+    const u64 wi = (u64)n * (ent[i] >> 32);
     if (wi < A) {
       ++nl;
       dl += A - wi;
@@ -172,7 +171,7 @@ __device__ void alias_build_block(const u64* wq, const uint16_t* key, u32 n, u64
   u64 oh = block_excl_scan_u64(nh, sh, &nH);
   u64 oe = block_excl_scan_u64(eh, sh, &Etot);
   for (u32 i = i0; i < i1; ++i) {
-    const u64 wi = (u64)n * wq[i];
+    const u64 wi = (u64)n * (ent[i] >> 32);
     if (wi < A) {
       vals[ol] = od;
       idx[ol] = (uint16_t)i;
@@ -188,6 +187,7 @@ __device__ void alias_build_block(const u64* wq, const uint16_t* key, u32 n, u64
   __syncthreads();
   const u64* Ev = vals + nL;
   const uint16_t* Hi = idx + nL;
+  auto key = [&](u32 i) -> u64 { return ent[i] & 0xffffu; };
   for (u32 i = tid; i < (u32)nL; i += NT) {
     const u64 D = vals[i];
     u32 lo = 0, hi = (u32)nH - 1;  // first j with E_j >= D (exists: D < Dtot = E_last)
@@ -196,7 +196,7 @@ __device__ void alias_build_block(const u64* wq, const uint16_t* key, u32 n, u64
       if (Ev[mid] >= D) hi = mid; else lo = mid + 1;
     }
     const u32 l = idx[i];
-    out[l] = ((u64)key[Hi[lo]] << 48) | ((u64)key[l] << 32) | alias_threshold((u64)n * wq[l], A);
+    out[l] = (key(Hi[lo]) << 48) | (key(l) << 32) | alias_threshold((u64)n * (ent[l] >> 32), A);
   }
   for (u32 j = tid; j < (u32)nH; j += NT) {
     const u32 h = Hi[j];
@@ -207,48 +207,62 @@ __device__ void alias_build_block(const u64* wq, const uint16_t* key, u32 n, u64
         const u32 mid = (lo + hi + 1) >> 1;
         if (vals[mid] <= E) lo = mid; else hi = mid - 1;
       }
-      const u64 d = A - (u64)n * wq[idx[lo]];
+      const u64 d = A - (u64)n * (ent[idx[lo]] >> 32);
       const u64 over = vals[lo] + d - E;
-      out[h] = ((u64)key[Hi[j + 1]] << 48) | ((u64)key[h] << 32) | alias_threshold(A - over, A);
+      out[h] = (key(Hi[j + 1]) << 48) | (key(h) << 32) | alias_threshold(A - over, A);
     } else {
-      out[h] = ((u64)key[h] << 48) | ((u64)key[h] << 32) | 0xffffffffu;
+      out[h] = (key(h) << 48) | (key(h) << 32) | 0xffffffffu;
     }
   }
 }
 
 // Per word: q = floor(x * 2^32 / S[k]) (clamped) written back densely; the
-// word's topics with q > 0 compacted in ascending order (nnz, the per-word
-// list q << 32 | k, the dense mass A) and the sparse alias table over them.
-// Persistent blocks loop over words; scratch is shared memory or, for large
-// K, a per-block slice of global memory.
+// word's topics with q > 0 compacted in ascending order into its list
+// (q << 32 | k, which is also the alias build's input), the dense mass A, nnz,
+// and the sparse alias table over the list.  The dense pass gives each thread
+// kPerThread consecutive topics per tile, so a tile needs one block scan.
+// The alias build's scratch (10 bytes per nonzero) is shared memory when the
+// word's nonzeros fit smem_items, else the block's slice of global scratch.
+constexpr u32 kPerThread = 8;
+
 __device__ __forceinline__ void alias_word(u32 K, u32* __restrict__ qrow, const u64* __restrict__ S, u64* alrow,
-                                           u64* csrrow, u64* A_out, u32* nnz_out, u64* cq, u64* vals, uint16_t* ck,
-                                           uint16_t* idx, u64* sh) {
+                                           u64* csrrow, u64* A_out, u32* nnz_out, u64* s_vals, uint16_t* s_idx,
+                                           u32 smem_items, u64* g_vals, uint16_t* g_idx, u64* sh) {
   u64 part = 0, nz = 0;
-  for (u32 t0 = 0; t0 < K; t0 += blockDim.x) {
-    const u32 k = t0 + threadIdx.x;
-    u64 qq = 0;
-    if (k < K) {
-      const u32 x = qrow[k];
-      if (x) {
-        qq = (((u64)x) << 32) / S[k];
-        if (qq > 0xffffffffULL) qq = 0xffffffffULL;
+  const u32 tile = blockDim.x * kPerThread;
+  for (u32 t0 = 0; t0 < K; t0 += tile) {
+    const u32 k0 = t0 + threadIdx.x * kPerThread;
+    u32 qv[kPerThread];
+    u32 cnt = 0;
+#pragma unroll
+    for (u32 c = 0; c < kPerThread; ++c) {
+      const u32 k = k0 + c;
+      u64 qq = 0;
+      if (k < K) {
+        const u32 x = qrow[k];
+        if (x) {
+          qq = (((u64)x) << 32) / S[k];
+          if (qq > 0xffffffffULL) qq = 0xffffffffULL;
+        }
+        qrow[k] = (u32)qq;
       }
-      qrow[k] = (u32)qq;
+      qv[c] = (u32)qq;
+      cnt += qq != 0;
+      part += qq;
     }
-    u64 tile;
-    const u64 pos = nz + block_excl_scan_u64(qq != 0, sh, &tile);
-    if (qq) {
-      cq[pos] = qq;
-      ck[pos] = (uint16_t)k;
-    }
-    nz += tile;
-    part += qq;
+    u64 tot;
+    u64 pos = nz + block_excl_scan_u64(cnt, sh, &tot);
+#pragma unroll
+    for (u32 c = 0; c < kPerThread; ++c)
+      if (qv[c]) csrrow[pos++] = ((u64)qv[c] << 32) | (k0 + c);
+    nz += tot;
   }
-  const u64 A = block_sum_u64(part, sh);  // (also a barrier for cq/ck)
+  const u64 A = block_sum_u64(part, sh);  // (also orders the list writes before the build)
   const u32 n = (u32)nz;
-  for (u32 i = threadIdx.x; i < n; i += blockDim.x) csrrow[i] = (cq[i] << 32) | ck[i];
-  if (n) alias_build_block(cq, ck, n, A, vals, idx, alrow, sh);
+  if (n) {
+    const bool in_smem = n <= smem_items;
+    alias_build_block(csrrow, n, A, in_smem ? s_vals : g_vals, in_smem ? s_idx : g_idx, alrow, sh);
+  }
   if (threadIdx.x == 0) {
     *A_out = A;
     *nnz_out = n;
@@ -256,18 +270,19 @@ __device__ __forceinline__ void alias_word(u32 K, u32* __restrict__ qrow, const 
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) alias_build_kernel(ModelDev m, unsigned char* gscratch, size_t slice) {
+__global__ void __launch_bounds__(256) alias_build_kernel(ModelDev m, unsigned char* gscratch, size_t slice,
+                                                          u32 smem_items) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   __shared__ u64 sh[33];
   const u32 K = m.K;
-  unsigned char* base = gscratch ? gscratch + (size_t)blockIdx.x * slice : s_raw;
-  u64* cq = (u64*)base;        // compacted weights
-  u64* vals = cq + K;
-  uint16_t* ck = (uint16_t*)(vals + K);  // compacted topics
-  uint16_t* idx = ck + K;
+  u64* s_vals = (u64*)s_raw;
+  uint16_t* s_idx = (uint16_t*)(s_vals + smem_items);
+  u64* g_vals = gscratch ? (u64*)(gscratch + (size_t)blockIdx.x * slice) : nullptr;
+  uint16_t* g_idx = gscratch ? (uint16_t*)(g_vals + K) : nullptr;
   for (u32 w = blockIdx.x; w < m.V; w += gridDim.x) {
     const size_t row = (size_t)w * K;
-    alias_word(K, m.q + row, m.S, m.al + row, m.csr + row, m.A + w, m.nnz + w, cq, vals, ck, idx, sh);
+    alias_word(K, m.q + row, m.S, m.al + row, m.csr + row, m.A + w, m.nnz + w, s_vals, s_idx, smem_items, g_vals,
+               g_idx, sh);
   }
 }
 
@@ -276,15 +291,13 @@ __global__ void __launch_bounds__(256) alias_build_kernel(ModelDev m, unsigned c
 __global__ void __launch_bounds__(256) alias_build_batch_kernel(ModelDev ar, BatchPhiDev bp, u32 Kmax, u32 w0, u32 w1) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   __shared__ u64 sh[33];
-  u64* cq = (u64*)s_raw;
-  u64* vals = cq + Kmax;
-  uint16_t* ck = (uint16_t*)(vals + Kmax);
-  uint16_t* idx = ck + Kmax;
+  u64* vals = (u64*)s_raw;
+  uint16_t* idx = (uint16_t*)(vals + Kmax);
   for (u32 w = w0 + blockIdx.x; w < w1; w += gridDim.x) {
     const u32 pb = bp.wpid[w], K = bp.K[pb];
     const size_t row = bp.row_off[w];
-    alias_word(K, ar.q + row, ar.S + bp.S_off[pb], ar.al + row, ar.csr + row, ar.A + w, ar.nnz + w, cq, vals, ck,
-               idx, sh);
+    alias_word(K, ar.q + row, ar.S + bp.S_off[pb], ar.al + row, ar.csr + row, ar.A + w, ar.nnz + w, vals, idx, Kmax,
+               nullptr, nullptr, sh);
   }
 }
 
@@ -294,18 +307,16 @@ __global__ void bump_kernel(u32* t) { *t += 1; }
 __global__ void debug_alias_kernel(const u32* q, u32 K, u64* out) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   __shared__ u64 sh[33];
-  u64* sq = (u64*)s_raw;
-  u64* vals = sq + K;
-  uint16_t* key = (uint16_t*)(vals + K);
-  uint16_t* idx = key + K;
+  u64* ent = (u64*)s_raw;  // (q << 32 | item)
+  u64* vals = ent + K;
+  uint16_t* idx = (uint16_t*)(vals + K);
   u64 part = 0;
   for (u32 k = threadIdx.x; k < K; k += blockDim.x) {
-    sq[k] = q[k];
-    key[k] = (uint16_t)k;
+    ent[k] = ((u64)q[k] << 32) | k;
     part += q[k];
   }
   const u64 A = block_sum_u64(part, sh);
-  alias_build_block(sq, key, K, A, vals, idx, out, sh);
+  alias_build_block(ent, K, A, vals, idx, out, sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -349,7 +360,7 @@ __global__ void debug_poisson_kernel(ModelDev m, const u32* count, const u64* id
 }  // namespace
 
 static u32 alias_threads(u32 K);
-static size_t alias_smem_bytes(u32 K);
+static size_t alias_scratch_item_bytes(u32 n);
 
 int device_sm_count() {
   static int sms = 0;
@@ -384,7 +395,7 @@ void launch_phi_draw_batch(const ModelDev& ar, const BatchPhiDev& bp, u32 n_bloc
 void launch_alias_build_batch(const ModelDev& ar, const BatchPhiDev& bp, u32 Kmax, u32 w0, u32 w1, cudaStream_t s) {
   if (w1 <= w0) return;
   const u32 nt = alias_threads(Kmax);
-  const size_t need = alias_smem_bytes(Kmax);
+  const size_t need = alias_scratch_item_bytes(Kmax);
   if (need > 48 * 1024) cudaFuncSetAttribute(alias_build_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, alias_build_batch_kernel, nt, need);
@@ -411,28 +422,37 @@ static u32 alias_threads(u32 K) {
   return 32 * nw;
 }
 
-static size_t alias_smem_bytes(u32 K) { return ((size_t)K * 20 + 15) & ~(size_t)15; }
+// Alias-build scratch for n items: vals (u64) then idx (u16), 16-byte rounded.
+static size_t alias_scratch_item_bytes(u32 n) { return ((size_t)n * 10 + 15) & ~(size_t)15; }
 
-constexpr size_t kMaxDynSmem = 200 * 1024;
+// Items whose scratch the solo alias kernel keeps in shared memory; words with
+// more nonzeros use the block's slice of global scratch.  Small shared memory
+// keeps several blocks resident per SM at any K.
+constexpr u32 kAliasSmemItems = 2048;
+constexpr u32 kAliasBlocksPerSm = 4;
+
+static size_t alias_slice_bytes(u32 K) { return (alias_scratch_item_bytes(K) + 255) & ~(size_t)255; }
 
 size_t alias_build_scratch_bytes(u32 K) {
-  if (alias_smem_bytes(K) <= kMaxDynSmem) return 0;
-  return alias_smem_bytes(K) * (size_t)device_sm_count() * 2;
+  if (K <= kAliasSmemItems) return 0;
+  return alias_slice_bytes(K) * (size_t)device_sm_count() * kAliasBlocksPerSm;
 }
 
 void launch_alias_build(const ModelDev& m, cudaStream_t s, void* scratch, size_t scratch_bytes) {
   const u32 nt = alias_threads(m.K);
-  const size_t need = alias_smem_bytes(m.K);
-  if (need <= kMaxDynSmem) {
-    if (need > 48 * 1024) cudaFuncSetAttribute(alias_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, alias_build_kernel, nt, need);
-    if (per_sm < 1) per_sm = 1;
-    const u32 blocks = std::min<u32>(m.V, (u32)(device_sm_count() * per_sm * 4));
-    alias_build_kernel<<<blocks, nt, need, s>>>(m, nullptr, 0);
+  const u32 items = std::min(m.K, kAliasSmemItems);
+  const size_t smem = alias_scratch_item_bytes(items);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, alias_build_kernel, nt, smem);
+  if (per_sm < 1) per_sm = 1;
+  u32 blocks = std::min<u32>(m.V, (u32)(device_sm_count() * per_sm * (m.K <= kAliasSmemItems ? 4 : 1)));
+  if (m.K > kAliasSmemItems) {
+    const size_t slice = alias_slice_bytes(m.K);
+    blocks = std::min<u32>(blocks, (u32)(scratch_bytes / slice));
+    if (!blocks) return;  // no scratch: the caller allocates alias_build_scratch_bytes(K)
+    alias_build_kernel<<<blocks, nt, smem, s>>>(m, (unsigned char*)scratch, slice, items);
   } else {
-    const u32 blocks = std::min<u32>(m.V, (u32)(scratch_bytes / need));
-    alias_build_kernel<<<blocks, nt, 0, s>>>(m, (unsigned char*)scratch, need);
+    alias_build_kernel<<<blocks, nt, smem, s>>>(m, nullptr, 0, items);
   }
 }
 
@@ -453,7 +473,7 @@ void launch_debug_poisson(const ModelDev& m, const u32* count, const u64* idx, u
 }
 
 void launch_debug_alias(const u32* q, u32 K, u64* out, cudaStream_t s) {
-  const size_t need = alias_smem_bytes(K);
+  const size_t need = (size_t)K * 8 + alias_scratch_item_bytes(K);
   if (need > 48 * 1024) cudaFuncSetAttribute(debug_alias_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
   debug_alias_kernel<<<1, alias_threads(K), need, s>>>(q, K, out);
 }
