@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--serve-unbatched", type=int, default=3000, help="serve: requests of the unbatched run")
     p.add_argument("--serve-train", type=int, default=5, help="serve: training iterations of the model")
     p.add_argument("--serve-slots", type=int, default=32, help="serve: launches in flight")
+    p.add_argument("--shard", action="store_true",
+                   help="one chain with its documents sharded across the ranks (strong scaling; default: replicas)")
     return p.parse_args()
 
 
@@ -577,6 +579,54 @@ def run_serve(args):
         print(json.dumps(line), flush=True)
 
 
+def run_sharded(args):
+    """One chain, documents sharded across the ranks by token-balanced ranges;
+    after every iteration the ranks add their count tables (NCCL all-reduce),
+    so the chain equals the single-GPU chain.  value = corpus tokens per
+    second of the whole job (strong scaling)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import gpupolyaurnlda_b200 as g
+    from gpupolyaurnlda_b200.shard import LibraryShard, ShardedChain, shard_ranges
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                            **({} if "MASTER_ADDR" in os.environ else
+                               {"init_method": "tcp://127.0.0.1:29533", "rank": 0, "world_size": 1}))
+    c = make_corpus(args, f"cuda:{local}")
+    sh = shard_ranges(c.d_len, world)[rank]
+    s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=0)
+    chain = ShardedChain(LibraryShard(s, c.z, c.w, c.d_len, sh))
+    chain.iterate(args.warmup)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    chain.iterate(args.steps)
+    torch.cuda.synchronize()
+    el = max_over_ranks(time.perf_counter() - t0, f"cuda:{local}")
+    clk = clocks.stop()
+    s.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": c.n_tokens * args.steps / el, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u64",
+                "data": "synthetic",
+                "config": dict(workload_desc(c, args), parallelism=f"document shards x{world} + count all-reduce"),
+                "timing": "wall clock around the timed iterations (each ends with a host synchronisation), max over "
+                          "ranks", "clocks": clk}
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -585,6 +635,8 @@ def main():
         run_batched(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.shard:
+        run_sharded(args)
     else:
         run_ours(args)
 

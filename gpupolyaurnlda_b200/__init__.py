@@ -125,6 +125,8 @@ _SIGNATURES = {
     "gpulda_initialize_ex": (C.c_int, [C.POINTER(Args), C.POINTER(Buffer), C.c_uint32, C.POINTER(ExArgs)]),
     "gpulda_set_stream": (C.c_int, [C.c_void_p]),
     "gpulda_pin_host": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32]),
+    "gpulda_set_token_offset": (C.c_int, [C.c_uint64]),
+    "gpulda_count_table": (C.c_int, [C.POINTER(C.c_void_p), _U64P]),
     "gpulda_unpin_host": (C.c_int, [C.c_void_p]),
     "gpulda_loglik": (C.c_int, [_F64P, _U64P]),
     "gpulda_corpus_load": (C.c_int, [_U32P, _U32P, _U32P, C.c_uint32, C.c_uint64]),
@@ -280,6 +282,23 @@ class Sampler:
 
     def set_stream(self, handle: int) -> None:
         check(self.L.gpulda_set_stream(C.c_void_p(handle)), "set_stream")
+
+    def set_token_offset(self, first_token: int) -> None:
+        """Global index of this process's first token (document sharding)."""
+        check(self.L.gpulda_set_token_offset(first_token), "set_token_offset")
+
+    def count_table(self):
+        """The device count table n (K*V uint32, word-major) as a CUDA int32
+        tensor sharing its memory (for an in-place all-reduce)."""
+        import torch
+        ptr = C.c_void_p()
+        n = C.c_uint64()
+        check(self.L.gpulda_count_table(C.byref(ptr), C.byref(n)), "count_table")
+
+        class _Arr:
+            __cuda_array_interface__ = {"shape": (n.value,), "typestr": "<i4", "data": (ptr.value, False),
+                                        "version": 3, "strides": None}
+        return torch.as_tensor(_Arr(), device="cuda")
 
     def loglik(self) -> tuple[float, int]:
         v = C.c_double()

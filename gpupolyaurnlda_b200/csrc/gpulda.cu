@@ -104,7 +104,8 @@ struct Model {
   float alpha = 0, beta = 0;
   u32 key0 = 0, key1 = 0, flags = 0;
   int t = -1;           // current iteration (sample_phi calls - 1)
-  u64 tok_offset = 0;   // tokens swept so far in the current iteration
+  u64 tok_offset = 0;   // global index of the next buffer's first token in the current iteration
+  u64 shard_base = 0;   // global index of this process's first token (document sharding)
   bool swept = false;   // a sweep ran since the last sample_phi
 
   ModelDev dev{};
@@ -343,7 +344,7 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
 // Phi step on `s` without a host synchronisation.
 int phi_step_async(cudaStream_t s) {
   g.t += 1;
-  g.tok_offset = 0;
+  g.tok_offset = g.shard_base;
   g.swept = false;
   g.launches = 0;
   CK(cudaEventRecord(g.ev[0], s));
@@ -691,6 +692,21 @@ extern "C" int gpulda_unpin_host(void* p) {
     cudaGetLastError();
     return cuda_fail(e, "cudaHostUnregister");
   }
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_set_token_offset(uint64_t first_token) {
+  if (!g.live) return fail(GPULDA_ERR_STATE, "set_token_offset before initialize");
+  g.shard_base = first_token;
+  g.tok_offset = first_token;
+  return GPULDA_OK;
+}
+
+extern "C" int gpulda_count_table(void** device_ptr, uint64_t* n_cells) {
+  if (!g.live) return fail(GPULDA_ERR_STATE, "count_table before initialize");
+  if (!device_ptr || !n_cells) return fail(GPULDA_ERR_ARGS, "null output");
+  *device_ptr = g.dev.n;
+  *n_cells = (uint64_t)g.K * g.V;
   return GPULDA_OK;
 }
 

@@ -174,6 +174,20 @@ int gpulda_kernel_times(float* ms, int n);
  * [4] kernels launched by the library in that iteration. */
 int gpulda_counters(uint64_t* out, int n);
 
+/* Document sharding across processes, one GPU each.  Every process holds the
+ * whole model (same arguments, seed and chain) and sweeps only its own range
+ * of documents.  gpulda_set_token_offset gives the global index, in the whole
+ * corpus, of the process's first token: the numbering of the next buffer and
+ * of every later iteration (after each sample_phi) starts there, so each token
+ * gets the draws the single-process chain gives it.  After its sweeps, the
+ * processes add their count tables in place (gpulda_count_table: the device
+ * array n, K*V uint32, e.g. an all-reduce sum over NCCL) before any of them
+ * calls sample_phi again; every process then computes the same Phi, and the
+ * chain equals the single-process chain bit for bit.  Log-likelihoods add
+ * likewise (gpulda_loglik returns the process's part). */
+int gpulda_set_token_offset(uint64_t first_token);
+int gpulda_count_table(void** device_ptr, uint64_t* n_cells);
+
 /* Page-locks (pins) a host range so the copies of sample_z_async / sync_buffer
  * from and to it run as asynchronous DMA; e.g. the memory-mapped z/w/d/K_d
  * files of a streaming host loop.  GPULDA_PIN_READ_ONLY for ranges mapped
