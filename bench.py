@@ -14,10 +14,16 @@ every token and rebuilds the counts.  Default workload: the mid configuration
           sparse work counted by the kernel) over its CUDA-event time,
           against the measured HBM copy bandwidth
   cpu_baseline  the CPU oracle (same algorithm) on a bounded sample, all cores
+  serving  fold-in requests against the trained model at 1k and 50k docs/s
+          offered: continuous batching vs one launch per document
 
 --impl reference times the CPU oracle alone (the reference has no CPU
-implementation of the path and its CUDA kernels are not run).
-Multi-GPU (torchrun): independent chains per GPU (replicas), weak scaling.
+implementation of the path, and its CUDA kernels do not build for sm_100a).
+Multi-GPU (torchrun): independent chains per GPU (replicas), weak scaling;
+--shard: one chain with its documents sharded across the GPUs.
+Other workloads: --workload batched (64 independent problems in one graph),
+--workload serve (the serving comparison at several rates), large_k1000,
+large_k10000.
 """
 from __future__ import annotations
 
@@ -48,6 +54,7 @@ def parse():
     p.add_argument("--docs", type=int, default=None, help="override the number of documents")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU seconds per timed oracle iteration")
     p.add_argument("--problems", type=int, default=64, help="batched workload: number of problems")
     p.add_argument("--batch-scale", type=float, default=1.0, help="batched workload: scale of each problem's D")
@@ -295,7 +302,28 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     s.set_stream(0)
-    s.close()
+
+    # ---- serving fold-in against the model just trained (one GPU) ----------
+    serving = None
+    if world == 1 and not args.no_serve and c.K <= 2048:
+        from gpupolyaurnlda_b200.serve import Server
+        srv_b = Server(50, seed=0, max_inflight=1 << 17)
+        srv_u = Server(50, mode="launch", slots=args.serve_slots, max_batch=1, seed=0)
+        s.close()
+        rows, ll = serve_measure(srv_b, srv_u, [1000, 50000], 2.0, 100000, 3000, local)
+        srv_b.close()
+        srv_u.close()
+        serving = {"metric": "served_docs_per_sec", "unit": "docs/s",
+                   "workload": f"the chain's model after {args.warmup + args.steps} iterations, {SERVE_WORKLOAD}; "
+                               f"batched = persistent kernel (32 request warps per SM), unbatched = one launch per "
+                               f"document over {args.serve_slots} streams",
+                   "rates": [{"offered": r["offered_docs_per_sec"], "requests": r["requests"],
+                              "batched": r["batched"], "unbatched": r["unbatched"],
+                              "speedup": r["batched"]["docs_per_sec"] / r["unbatched"]["docs_per_sec"],
+                              "results_identical": r["results_identical"]} for r in rows],
+                   "heldout_ll_per_token": ll}
+    else:
+        s.close()
 
     value = replica_value(c.n_tokens, args.steps, world, ms_max / 1e3)
     zb = [24 * c.n_tokens + 8 * c.n_docs + 4 * S for S in S_work]
@@ -342,12 +370,14 @@ def run_ours(args):
                              "traffic": (tpt * c.n_tokens if (tpt := measured_traffic_per_token()) else None),
                              "traffic_note": "ncu dram bytes per token of a 3.4e7-token slice, scaled to N",
                              "kernel": "z_sweep_kernel",
+                             "binding_resource": "L1 data pipe (84-89 % of wavefront slots in the ncu profile); "
+                                                 "DRAM at 2.4 %: most gathers hit L2",
                              "algorithmic_bytes_per_launch": float(np.mean(zb)), "peak_kind": peak_kind},
                 "iteration_roofline": {"achieved": it_gbs, "frac": it_gbs / hbm,
                                        "bytes_per_iteration": float(np.mean(B_iter))},
                 "kernel_ms": {"z_sweep": float(np.mean(z_ms)), "phi_step": float(np.mean(phi_ms))},
                 "sparse_work_per_token": float(np.mean(S_work)) / c.n_tokens,
-                "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cpu}
+                "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -506,33 +536,15 @@ def serve_open_loop(srv, lengths, words, arrival_s, ids):
     return n / ((last - arr[0]) / 1e9), lat, ll, sk
 
 
-def run_serve(args):
-    """Serving fold-in: a K=1000, V=100000 model trained on the mid corpus is
-    served to Poisson arrivals of Zipf documents (lengths lognormal(5.0, 1.2)
-    clipped to [5, 20000]), 50 fold-in iterations each; continuous batching
-    against one launch per document on the same request streams."""
-    import torch
-
-    import gpupolyaurnlda_b200 as g
-    from gpupolyaurnlda_b200 import corpus
-    from gpupolyaurnlda_b200.serve import Server, zipf_requests
-
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    c = corpus.generate("mid", seed=1, device=f"cuda:{local}")
-    s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=0)
-    s.corpus_load(c.z.copy(), c.w, c.d_len)
-    s.corpus_sweep(args.serve_train)
-    n_iter = 50
-    srv_b = Server(n_iter, seed=0, max_inflight=1 << 17)  # persistent: 32 request warps per SM
-    srv_u = Server(n_iter, mode="launch", slots=args.serve_slots, max_batch=1, seed=0)
-    s.close()
-    del c
+def serve_measure(srv_b, srv_u, rates, seconds, max_requests, max_unbatched, local):
+    """Open-loop serving runs at the given offered rates against the batched
+    (persistent) and the one-launch-per-document servers; returns the per-rate
+    rows and the held-out log-likelihood per token of both (same requests)."""
+    from gpupolyaurnlda_b200.serve import zipf_requests
     rows = []
     ll_b_all, ll_u_all, tok_all = [], [], []
-    for rate in args.rates:
-        n = int(min(max(args.serve_seconds * rate, 2000), args.serve_requests))
+    for rate in rates:
+        n = int(min(max(seconds * rate, 2000), max_requests))
         lengths, words = zipf_requests(n, srv_b.V, seed=rate)
         rng = np.random.default_rng(rate + 1)
         arrival = np.cumsum(rng.exponential(1.0 / rate, n))
@@ -541,7 +553,7 @@ def run_serve(args):
         clocks.start()
         dps_b, lat_b, ll_b, sk_b = serve_open_loop(srv_b, lengths, words, arrival, ids)
         clk = clocks.stop()
-        nu = min(n, args.serve_unbatched)
+        nu = min(n, max_unbatched)
         dps_u, lat_u, ll_u, sk_u = serve_open_loop(srv_u, lengths[:nu], words[:int(lengths[:nu].sum())],
                                                    arrival[:nu], ids[:nu])
         same = bool((ll_b[:nu] == ll_u).all() and (sk_b[:nu] == sk_u).all())
@@ -555,27 +567,55 @@ def run_serve(args):
                                    "p50_ms": float(np.percentile(lat_u, 50) / 1e6),
                                    "p99_ms": float(np.percentile(lat_u, 99) / 1e6)},
                      "results_identical": same, "clocks": clk})
+    llb, llu = sum(ll_b_all) / sum(tok_all), sum(ll_u_all) / sum(tok_all)
+    return rows, {"batched": llb, "unbatched": llu, "rel_diff": abs(llb - llu) / abs(llu)}
+
+
+SERVE_WORKLOAD = ("50 fold-in iterations per request, Zipf(1.05) documents, lengths lognormal(5.0,1.2) clipped "
+                  "[5,20000], Poisson arrivals")
+
+
+def run_serve(args):
+    """Serving fold-in: a K=1000, V=100000 model trained on the mid corpus is
+    served to Poisson arrivals of Zipf documents (lengths lognormal(5.0, 1.2)
+    clipped to [5, 20000]), 50 fold-in iterations each; continuous batching
+    against one launch per document on the same request streams."""
+    import torch
+
+    import gpupolyaurnlda_b200 as g
+    from gpupolyaurnlda_b200 import corpus
+    from gpupolyaurnlda_b200.serve import Server
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    c = corpus.generate("mid", seed=1, device=f"cuda:{local}")
+    s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=0)
+    s.corpus_load(c.z.copy(), c.w, c.d_len)
+    s.corpus_sweep(args.serve_train)
+    srv_b = Server(50, seed=0, max_inflight=1 << 17)  # persistent: 32 request warps per SM
+    srv_u = Server(50, mode="launch", slots=args.serve_slots, max_batch=1, seed=0)
+    s.close()
+    del c
+    rows, ll = serve_measure(srv_b, srv_u, args.rates, args.serve_seconds, args.serve_requests,
+                             args.serve_unbatched, local)
     st_b = srv_b.stats()
     srv_b.close()
     srv_u.close()
     top = rows[-1]
-    llb, llu = sum(ll_b_all) / sum(tok_all), sum(ll_u_all) / sum(tok_all)
     if rank == 0:
         line = {"metric": "served_docs_per_sec", "value": top["batched"]["docs_per_sec"], "unit": "docs/s",
                 "n_gpus": 1, "steps": len(rows), "warmup": 0,
                 "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "u64", "data": "synthetic",
                 "config": {"workload": f"serving fold-in: K=1000 V=100000 model (mid corpus, {args.serve_train} "
-                                       f"training iterations), {n_iter} fold-in iterations per request, Zipf(1.05) "
-                                       f"documents, lengths lognormal(5.0,1.2) clipped [5,20000], Poisson arrivals "
-                                       f"at {list(args.rates)} docs/s",
+                                       f"training iterations), {SERVE_WORKLOAD} at {list(args.rates)} docs/s",
                            "batched": "persistent kernel, 32 request warps per SM",
                            "unbatched": f"one launch per document, {args.serve_slots} streams"},
                 "p50_ms": top["batched"]["p50_ms"], "p99_ms": top["batched"]["p99_ms"],
                 "unbatched": top["unbatched"],
                 "speedup_vs_unbatched": top["batched"]["docs_per_sec"] / top["unbatched"]["docs_per_sec"],
-                "heldout_ll_per_token": {"batched": llb, "unbatched": llu, "rel_diff": abs(llb - llu) / abs(llu)},
-                "rates": rows, "server_stats": st_b}
+                "heldout_ll_per_token": ll, "rates": rows, "server_stats": st_b}
         print(json.dumps(line), flush=True)
 
 
