@@ -285,6 +285,7 @@ def run_ours(args):
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     z_ms, phi_ms, S_work, launches = [], [], [], 0
+    draw_ms, alias_ms = [], []
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.steps):
@@ -293,6 +294,8 @@ def run_ours(args):
         cnt = s.counters()
         z_ms.append(kt["z_sweep"])
         phi_ms.append(kt["phi_draw"] + kt["alias_build"] + kt["prep"])
+        draw_ms.append(kt["phi_draw"])
+        alias_ms.append(kt["alias_build"])
         S_work.append(cnt["sparse_work"])
         launches += cnt["launches"]
     e1.record(stream)
@@ -302,6 +305,7 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     s.set_stream(0)
+    nnz_total = int(s.read_state(n=False, q=False, alias=False, A=False, S=False)["nnz"].astype(np.int64).sum())
 
     # ---- serving fold-in against the model just trained (one GPU) ----------
     serving = None
@@ -376,6 +380,13 @@ def run_ours(args):
                 "iteration_roofline": {"achieved": it_gbs, "frac": it_gbs / hbm,
                                        "bytes_per_iteration": float(np.mean(B_iter))},
                 "kernel_ms": {"z_sweep": float(np.mean(z_ms)), "phi_step": float(np.mean(phi_ms))},
+                "kernel_gbs": {
+                    "note": "algorithmic bytes / CUDA-event time per kernel: Poisson draw 12 B per (word, topic) "
+                            "cell (read n, write x, zero n); alias build 8 B per cell + 16 B per nonzero Phi "
+                            "(list and alias entry); z sweep as in roofline (the count rebuild is its atomics)",
+                    "phi_draw": 12 * c.K * c.V / (float(np.mean(draw_ms)) / 1e3) / 1e9,
+                    "alias_build": (8 * c.K * c.V + 16 * nnz_total) / (float(np.mean(alias_ms)) / 1e3) / 1e9,
+                    "z_sweep": z_gbs},
                 "sparse_work_per_token": float(np.mean(S_work)) / c.n_tokens,
                 "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving}
         print(json.dumps(line), flush=True)
