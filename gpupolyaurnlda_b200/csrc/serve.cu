@@ -78,6 +78,10 @@ struct FoldReq {
 };
 static_assert(sizeof(FoldReq) == 32, "FoldReq");
 
+// Shared memory per request warp: the document's counts and the staged
+// per-token data of a 32-token chunk.
+inline size_t fold_smem_bytes(u32 K) { return doc_counts_bytes(K) + 32 * 32; }
+
 // Output record of a request: theta[K] (float), then 8-byte aligned the
 // log-likelihood (double), skipped tokens (u32) and the done flag (u32).
 __host__ __device__ inline size_t ll_offset(u32 K) { return (size_t)K * 4 + ((K & 1) ? 4 : 0); }
@@ -102,7 +106,7 @@ constexpr u32 kStatusBadRequest = 16;
 // Fold-in of one request by one warp.  Words are read through L2 only: the
 // pool is refilled by copies while kernels run, so an SM's L1 may still hold
 // an earlier request's words at the same address.
-__device__ void fold_request(const FoldCommon& a, DocCounts& dc, const FoldReq& rq, u32 lane) {
+__device__ void fold_request(const FoldCommon& a, DocCounts& dc, uint4* stage, const FoldReq& rq, u32 lane) {
   if (rq.w_off + rq.len > a.pool_words || rq.z_off + rq.len > a.pool_words || rq.rec >= a.n_recs ||
       rq.len > 65535u) {
     if (lane == 0) atomicOr(a.status, kStatusBadRequest);
@@ -142,13 +146,16 @@ __device__ void fold_request(const FoldCommon& a, DocCounts& dc, const FoldReq& 
       const u64 my_al = (valid && my_nw) ? __ldg(m.al + my_row + my_s) : 0ull;
       u32 new_z = my_z;
       const u32 nt = min(32u, L - base);
+      // per-token data staged in shared memory (broadcast loads, not shuffles)
+      __syncwarp();
+      stage[2 * lane] = make_uint4(my_z, r.x, r.y, my_nw);
+      stage[2 * lane + 1] = make_uint4((u32)my_row, (u32)(my_row >> 32), (u32)my_A, (u32)(my_A >> 32));
+      __syncwarp();
       for (u32 j = 0; j < nt; ++j) {
-        const u32 zj = __shfl_sync(kFullMask, my_z, j);
-        const u32 r0 = __shfl_sync(kFullMask, r.x, j);
-        const u32 r1 = __shfl_sync(kFullMask, r.y, j);
-        const size_t row = (size_t)__shfl_sync(kFullMask, my_row, j);
-        const u32 nw = __shfl_sync(kFullMask, my_nw, j);
-        const u64 Aw = __shfl_sync(kFullMask, my_A, j);
+        const uint4 s0 = stage[2 * j], s1 = stage[2 * j + 1];
+        const u32 zj = s0.x, r0 = s0.y, r1 = s0.z, nw = s0.w;
+        const size_t row = ((u64)s1.y << 32) | s1.x;
+        const u64 Aw = ((u64)s1.w << 32) | s1.z;
         u32 nzm;
         bool sp;
         const u32 k = token_step(dc, zj, r0, r1, r.w, my_al, j, m.q + row, m.csr + row, nw, Aw, alpha, lane, &nzm,
@@ -166,18 +173,28 @@ __device__ void fold_request(const FoldCommon& a, DocCounts& dc, const FoldReq& 
   float* theta = (float*)rec;
   const double denom = (double)L + (double)K * (double)alpha;
   for (u32 k = lane; k < K; k += 32) theta[k] = (float)(((double)dc.cnt[k] + (double)alpha) / denom);
+  // sum_k (m_k + alpha) q[w][k] = sum_k m_k q[w][k] + alpha A[w]: the first term
+  // exactly (u64) over the shorter of the two lists, the second from the dense mass
   double ll = 0.0;
   u32 skipped = 0;
   for (u32 i = 0; i < L; ++i) {
     const u32 wi = __ldcg(w + i) % V;
     const u32 nw = __ldg(m.nnz + wi);
-    const u64* crow = m.csr + (size_t)wi * K;
-    double s = 0.0;
-    for (u32 e = lane; e < nw; e += 32) {
-      const u64 ent = __ldg(crow + e);
-      s += ((double)dc.cnt[(u32)ent & 0xffffu] + (double)alpha) * (double)(u32)(ent >> 32);
+    const size_t row = (size_t)wi * K;
+    u64 part = 0;
+    if (nw < dc.nl) {
+      for (u32 e = lane; e < nw; e += 32) {
+        const u64 ent = __ldg(m.csr + row + e);
+        part += (u64)dc.cnt[(u32)ent & 0xffffu] * (u32)(ent >> 32);
+      }
+    } else {
+      for (u32 e = lane; e < dc.nl; e += 32) {
+        const u32 k = dc.tl[e];
+        part += (u64)dc.cnt[k] * __ldg(m.q + row + k);
+      }
     }
-    s = warp_sum_f64(s);
+    const u64 Bw = warp_sum_u64(part);
+    const double s = (double)Bw + (double)alpha * (double)__ldg(m.A + wi);
     if (s > 0.0)
       ll += log(s);
     else
@@ -202,8 +219,9 @@ __device__ void fold_request(const FoldCommon& a, DocCounts& dc, const FoldReq& 
 __global__ void __launch_bounds__(32) fold_launch_kernel(FoldCommon a, const FoldReq* items) {
   extern __shared__ __align__(16) unsigned char fsm[];
   DocCounts dc = doc_counts_at(fsm, a.m.K);
+  uint4* stage = reinterpret_cast<uint4*>(fsm + doc_counts_bytes(a.m.K));
   const FoldReq rq = items[blockIdx.x];
-  fold_request(a, dc, rq, threadIdx.x);
+  fold_request(a, dc, stage, rq, threadIdx.x);
 }
 
 struct RingDev {
@@ -248,6 +266,7 @@ __global__ void __launch_bounds__(32, 32) fold_persistent_kernel(FoldCommon a, R
   extern __shared__ __align__(16) unsigned char fsm[];
   const u32 lane = threadIdx.x;
   DocCounts dc = doc_counts_at(fsm, a.m.K);
+  uint4* stage = reinterpret_cast<uint4*>(fsm + doc_counts_bytes(a.m.K));
   while (true) {
     unsigned long long mine = ~0ull;
     if (lane == 0) {
@@ -286,7 +305,7 @@ __global__ void __launch_bounds__(32, 32) fold_persistent_kernel(FoldCommon a, R
     rq.rid = ((u64)hi.y << 32) | hi.x;
     rq.len = hi.z;
     rq.rec = hi.w;
-    fold_request(a, dc, rq, lane);
+    fold_request(a, dc, stage, rq, lane);
   }
 }
 
@@ -517,7 +536,7 @@ int create_common(const GpuldaServeArgs* a, u32 K, u32 V, float alpha, std::uniq
   SCK(cudaHostGetDevicePointer((void**)&fc.recs, s.recs_host, 0));
   s.free_recs.resize(s.max_inflight);
   for (u32 i = 0; i < s.max_inflight; ++i) s.free_recs[i] = s.max_inflight - 1 - i;
-  const size_t smem = doc_counts_bytes(K);
+  const size_t smem = fold_smem_bytes(K);
   if (s.persistent) {
     s.resident_per_sm = a->slots ? a->slots : 32u;
     s.ring_cap = 1;
@@ -639,9 +658,9 @@ int ensure_kernel(Server& s) {
   rd.tail = (const u64*)(s.ctl + 8);
   rd.stop = (const u32*)(s.ctl + 16);
   int fit = 0;
-  SCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fold_persistent_kernel, 32, doc_counts_bytes(s.K)));
+  SCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fold_persistent_kernel, 32, fold_smem_bytes(s.K)));
   const u32 blocks = (u32)device_sm_count() * std::max<u32>(1, std::min<u32>(s.resident_per_sm, (u32)fit));
-  fold_persistent_kernel<<<blocks, 32, doc_counts_bytes(s.K), s.kern_s>>>(s.fc, rd);
+  fold_persistent_kernel<<<blocks, 32, fold_smem_bytes(s.K), s.kern_s>>>(s.fc, rd);
   SCK(cudaGetLastError());
   SCK(cudaEventRecord(s.kern_ev, s.kern_s));
   s.kern_live = true;
@@ -721,7 +740,7 @@ int launch_batches(Server& s) {
     u32* items = s.fc.pool + off + 2 * align_up(std::max<u64>(T, 1), 64);
     if (T) SCK(cudaMemcpyAsync(s.fc.pool + off, sl.st.p + head, T * 4, cudaMemcpyHostToDevice, sl.s));
     SCK(cudaMemcpyAsync(items, sl.st.p + 16, n * sizeof(FoldReq), cudaMemcpyHostToDevice, sl.s));
-    fold_launch_kernel<<<(u32)n, 32, doc_counts_bytes(s.K), sl.s>>>(s.fc, (const FoldReq*)items);
+    fold_launch_kernel<<<(u32)n, 32, fold_smem_bytes(s.K), sl.s>>>(s.fc, (const FoldReq*)items);
     SCK(cudaGetLastError());
     SCK(cudaEventRecord(sl.done, sl.s));
     sl.busy = true;  // the staging buffer is reused once `done` has passed
