@@ -35,18 +35,29 @@ enum TimerSlot { kTPhi = 0, kTPrep = 1, kTAlias = 2, kTOffsets = 3, kTZ = 4, kTN
 // A buffer's sweep is split into this many pieces of about equal token counts
 // so that copying piece p+1 in and piece p-1 out overlaps sweeping piece p.
 constexpr u32 kPieces = 8;
+// A piece's documents of at least this many times its mean length are swept by
+// a separate launch on a high-priority stream: the block scheduler then starts
+// them as soon as their piece has arrived and a block slot frees, instead of
+// behind the earlier pieces' queues, so the longest sequential chains of the
+// last pieces do not set the sweep's tail.
+constexpr u32 kLongFactor = 4;
+
+constexpr u32 kWorkCounters = 2 + 2 * kPieces;
 
 struct BufCtx {
   cudaStream_t stream = nullptr;  // sweeps
   cudaStream_t h2d = nullptr, d2h = nullptr;
   cudaStream_t piece[kPieces] = {};  // one stream per piece, so piece sweeps overlap
+  cudaStream_t lpiece[kPieces] = {};  // high priority: each piece's long documents
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // [0] order copied, [1] last copy out issued
-  cudaEvent_t in[kPieces] = {}, out[kPieces] = {};
+  cudaEvent_t in[kPieces] = {}, out[kPieces] = {}, lout[kPieces] = {};
   cudaEvent_t offs = nullptr;     // document offsets of the current sweep are ready
   bool used = false;
   u32* order = nullptr;           // device: document processing order
-  // Device work counters of this buffer's launches (2 + kPieces), so sweeps
-  // of different buffers may be in flight at the same time.
+  // Device work counters of this buffer's launches (kWorkCounters), so sweeps
+  // of different buffers may be in flight at the same time: [0] whole buffer,
+  // [1, 1 + kPieces) pieces, [1 + kPieces] short documents beside a split sweep,
+  // [2 + kPieces, 2 + 2 kPieces) the pieces' long documents.
   u32* work = nullptr;
   std::vector<u32> order_host;    // host staging of the order
 };
@@ -314,18 +325,22 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
     CK(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
     for (auto& ps : ctx->piece) CK(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
+    int lo_prio = 0, hi_prio = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio));
+    for (auto& ps : ctx->lpiece) CK(cudaStreamCreateWithPriority(&ps, cudaStreamNonBlocking, hi_prio));
     for (auto& e : ctx->ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ctx->offs, cudaEventDisableTiming));
     for (u32 i = 0; i < kPieces; ++i) {
       CK(cudaEventCreateWithFlags(&ctx->in[i], cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&ctx->out[i], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&ctx->lout[i], cudaEventDisableTiming));
     }
     cudaStream_t* sp = new cudaStream_t(ctx->stream);
     b.stream = sp;
     b.gpu_rng = ctx;
     u32 *z, *w, *dl, *di, *kd;
     if ((rc = dalloc(&z, g.buffer_size)) || (rc = dalloc(&w, g.buffer_size)) || (rc = dalloc(&dl, g.max_D)) ||
-        (rc = dalloc(&di, g.max_D)) || (rc = dalloc(&kd, g.max_D)) || (rc = dalloc(&ctx->order, g.max_D)) || (rc = dalloc(&ctx->work, 2 + kPieces)))
+        (rc = dalloc(&di, g.max_D)) || (rc = dalloc(&kd, g.max_D)) || (rc = dalloc(&ctx->order, g.max_D)) || (rc = dalloc(&ctx->work, kWorkCounters)))
       return rc;
     b.gpu_z = z;
     b.gpu_w = w;
@@ -397,7 +412,7 @@ int z_launch(cudaStream_t s, u32* z, const u32* w, const u32* d_len, const u32* 
 }
 
 // With a split (large K), `order` lists the short documents first.
-// `work` holds 2 + kPieces zeroed-per-launch counters.
+// `work` holds kWorkCounters zeroed-per-launch counters.
 int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_idx, const u32* order, u32* K_d,
                  u32 n_docs, u64 n_tokens, bool offsets, cudaEvent_t* ev, u32* work, const DocSplit* split = nullptr) {
   CK(cudaEventRecord(ev[0], s));
@@ -460,9 +475,16 @@ int pipelined_sweep(Buffer* b, BufCtx* ctx) {
   if (ctx->used) CK(cudaEventSynchronize(ctx->ev[0]));
   ctx->order_host.resize(n);
   std::vector<u32> part;
+  u32 n_long[kPieces];
   for (u32 p = 0; p < kPieces; ++p) {
-    longest_first(b->d + dcut[p], dcut[p + 1] - dcut[p], part);
+    const u32 nd = dcut[p + 1] - dcut[p];
+    longest_first(b->d + dcut[p], nd, part);
     std::copy(part.begin(), part.end(), ctx->order_host.begin() + dcut[p]);
+    // the long documents are a prefix of the longest-first order
+    const u64 thr = nd ? (u64)kLongFactor * (tcut[p + 1] - tcut[p]) / nd : 0;
+    u32 nl = 0;
+    while (nl < nd && (u64)b->d[dcut[p] + part[nl]] >= thr && thr > 0) ++nl;
+    n_long[p] = nl;
   }
   u32* gz = (u32*)b->gpu_z;
   u32* gw = (u32*)b->gpu_w;
@@ -491,12 +513,22 @@ int pipelined_sweep(Buffer* b, BufCtx* ctx) {
     cudaStream_t ps = ctx->piece[p];
     CK(cudaStreamWaitEvent(ps, ctx->in[p], 0));
     CK(cudaStreamWaitEvent(ps, ctx->offs, 0));  // document offsets are ready
-    const u32 nd = dcut[p + 1] - dcut[p];
-    if (nd) {
-      const int rc = z_launch(ps, gz, gw, gdl + dcut[p], gdi + dcut[p], ctx->order + dcut[p], gkd + dcut[p], nd,
-                              b->n_tokens, tok_base, ctx->work + 1 + p);
+    const u32 nd = dcut[p + 1] - dcut[p], nl = n_long[p];
+    if (nl) {
+      cudaStream_t ls = ctx->lpiece[p];
+      CK(cudaStreamWaitEvent(ls, ctx->in[p], 0));
+      CK(cudaStreamWaitEvent(ls, ctx->offs, 0));
+      const int rc = z_launch(ls, gz, gw, gdl + dcut[p], gdi + dcut[p], ctx->order + dcut[p], gkd + dcut[p], nl,
+                              b->n_tokens, tok_base, ctx->work + 2 + kPieces + p);
+      if (rc) return rc;
+      CK(cudaEventRecord(ctx->lout[p], ls));
+    }
+    if (nd > nl) {
+      const int rc = z_launch(ps, gz, gw, gdl + dcut[p], gdi + dcut[p], ctx->order + dcut[p] + nl, gkd + dcut[p],
+                              nd - nl, b->n_tokens, tok_base, ctx->work + 1 + p);
       if (rc) return rc;
     }
+    if (nl) CK(cudaStreamWaitEvent(ps, ctx->lout[p], 0));
     CK(cudaEventRecord(ctx->out[p], ps));
     CK(cudaStreamWaitEvent(s, ctx->out[p], 0));
     CK(cudaStreamWaitEvent(ctx->d2h, ctx->out[p], 0));
@@ -635,11 +667,14 @@ extern "C" void cleanup(Buffer* buffers, uint32_t n_buffers) {
       for (u32 k = 0; k < kPieces; ++k) {
         if (ctx->in[k]) cudaEventDestroy(ctx->in[k]);
         if (ctx->out[k]) cudaEventDestroy(ctx->out[k]);
+        if (ctx->lout[k]) cudaEventDestroy(ctx->lout[k]);
       }
       if (ctx->stream) cudaStreamDestroy(ctx->stream);
       if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
       if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
       for (auto& ps : ctx->piece)
+        if (ps) cudaStreamDestroy(ps);
+      for (auto& ps : ctx->lpiece)
         if (ps) cudaStreamDestroy(ps);
       dfree(ctx->order);
       delete ctx;
