@@ -80,7 +80,9 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi samples during the timed region."""
+    """nvidia-smi samples (every 50 ms) during the timed region: start() returns
+    once the first sample has arrived, and stop() keeps the samples taken
+    between the two calls."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -94,30 +96,36 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.monotonic() + 5.0
+            while not self.rows and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t0 = time.monotonic()
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.monotonic(), [x.strip() for x in line.split(",")]))
 
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t1 = time.monotonic()
         self.proc.terminate()
         try:
             self.proc.wait(5)
         except Exception:
             self.proc.kill()
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        rows = [r for t, r in self.rows if self.t0 <= t <= t1] or [r for _, r in self.rows[-1:]]
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for r in self.rows:
+        for r in rows:
             if len(r) >= 9:
                 for nm, v in zip(names, r[5:9]):
                     if v.strip().lower() == "active":
@@ -279,10 +287,10 @@ def run_ours(args):
     for _ in range(args.warmup):
         s.corpus_sweep(1)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
+    if world > 1:
+        dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     z_ms, phi_ms, S_work, launches = [], [], [], 0
     draw_ms, alias_ms = [], []
@@ -441,10 +449,10 @@ def run_batched(args):
     info = b.info()
     b.sweep_async(args.warmup, stream.cuda_stream)
     b.sync()
-    if world > 1:
-        dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
+    if world > 1:
+        dist.barrier()
     torch.cuda.synchronize()
     e0.record(stream)
     b.sweep_async(args.steps, stream.cuda_stream)
@@ -656,9 +664,9 @@ def run_sharded(args):
     chain = ShardedChain(LibraryShard(s, c.z, c.w, c.d_len, sh))
     chain.iterate(args.warmup)
     torch.cuda.synchronize()
-    dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
+    dist.barrier()
     t0 = time.perf_counter()
     chain.iterate(args.steps)
     torch.cuda.synchronize()

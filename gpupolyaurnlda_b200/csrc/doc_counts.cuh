@@ -113,7 +113,6 @@ __device__ __forceinline__ void doc_counts_build(DocCounts& dc, const u32* z, u3
                                                  u32 bad_topic_bit) {
   const u32 Kp = (K + 63) & ~63u;
   for (u32 i = lane; i < Kp / 8; i += 32) reinterpret_cast<uint4*>(dc.cnt)[i] = make_uint4(0, 0, 0, 0);
-  for (u32 i = lane; i < Kp / 32; i += 32) dc.inl[i] = 0;
   __syncwarp();
   for (u32 i = lane; i < L; i += 32) {
     u32 k = z[i];
@@ -124,26 +123,21 @@ __device__ __forceinline__ void doc_counts_build(DocCounts& dc, const u32* z, u3
     atomicAdd(reinterpret_cast<u32*>(dc.cnt) + (k >> 1), 1u << ((k & 1) * 16));
   }
   __syncwarp();
-  // lane l compacts its contiguous range of topics
-  const u32 per = Kp / 32;
-  const u32 k0 = lane * per;
-  u32 c = 0;
-  for (u32 k = k0; k < k0 + per; ++k) c += dc.cnt[k] != 0;
-  u32 pos = c;
-#pragma unroll
-  for (u32 o = 1; o < 32; o <<= 1) {
-    const u32 y = __shfl_up_sync(kFullMask, pos, o);
-    if (lane >= o) pos += y;
+  // Sorted list and bitmap, 32 topics per round: lane l tests topic b + l
+  // (consecutive 16-bit loads, free of bank conflicts, where a contiguous
+  // range per lane would put the lanes' loads 64 bytes apart); the round's
+  // ballot is its bitmap word and gives each nonzero topic its list position.
+  const u32 below = (1u << lane) - 1u;
+  u32 pos = 0;
+  for (u32 b = 0; b < Kp; b += 32) {
+    const bool nz = dc.cnt[b + lane] != 0;
+    const u32 m = __ballot_sync(kFullMask, nz);
+    if (nz) dc.tl[pos + __popc(m & below)] = (uint16_t)(b + lane);
+    if (lane == 0) dc.inl[b >> 5] = m;
+    pos += __popc(m);
   }
-  dc.nz = __shfl_sync(kFullMask, pos, 31);
-  pos -= c;
-  for (u32 k = k0; k < k0 + per; ++k)
-    if (dc.cnt[k]) {
-      dc.tl[pos++] = (uint16_t)k;
-      atomicOr(dc.inl + (k >> 5), 1u << (k & 31));
-    }
   __syncwarp();
-  dc.nl = dc.nz;
+  dc.nz = dc.nl = pos;
 }
 
 // One token (lane j's in the current chunk): removes topic zj, draws the new

@@ -34,9 +34,19 @@ struct ZKernelArgs {
 // one set of arenas; each document's K, alpha, Philox key and token numbering
 // come from its problem, and a token's (word, topic) row starts at
 // b.row_off[w] instead of w * K.  Otherwise all parameters come from `m`.
-template <bool BATCH>
+//
+// LL: the launch accumulates the joint log-likelihood.  A separate
+// instantiation, so the sweep without it keeps no log-likelihood registers
+// live: the kernel runs at 64 registers per thread (four 256-thread blocks
+// per SM), where every live register is felt.  For the same reason the
+// statistics live in shared memory (per-chunk sums of at most 22 bits in one
+// register), not in per-thread 64-bit counters.
+template <bool BATCH, bool LL>
 __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
   extern __shared__ __align__(16) unsigned char zsm[];
+  __shared__ unsigned long long blk_stats[4];  // tokens, documents, sparse work, sparse draws
+  if (threadIdx.x < 4) blk_stats[threadIdx.x] = 0;
+  __syncthreads();
   const ModelDev& m = a.m;
   const ZLaunch& p = a.z;
   const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -44,9 +54,8 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
   unsigned char* wsm = zsm + (size_t)warp * (doc_counts_bytes(a.Kmax) + kTokStageBytes);
   DocCounts dc = doc_counts_at(wsm, a.Kmax);
   uint4* stage = reinterpret_cast<uint4*>(wsm + doc_counts_bytes(a.Kmax));
-  const bool want_ll = (p.flags & 1u) && p.ll;
+  const bool want_ll = LL;
 
-  u64 st_tok = 0, st_docs = 0, st_S = 0, st_sp = 0;
   // log-likelihood terms, accumulated per lane
   double ll_acc = 0.0, ll_skip = 0.0;
   u32 status = 0;
@@ -108,6 +117,9 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
       const u64 my_al = (valid && my_nw) ? __ldg(m.al + my_row + my_s) : 0ull;
       u32 new_z = my_z;
       const u32 nt = min(32u, L - base);
+      // sum over the chunk of (min(nz without the token, nnz[w]) << 6) + sparse
+      // (the first term at most 32 * 2048, the second at most 32)
+      u32 chunk_st = 0;
       // The chunk's per-token data is staged in shared memory and read back
       // with two 16-byte broadcast loads per token instead of eight
       // shuffles: shuffles and shared loads share the L1 data pipe, which
@@ -127,11 +139,14 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
                                  &sp);
         if (lane == 0) {
           atomicAdd(m.n + row + k, 1u);
-          st_S += min(nzm, nw);
-          st_sp += sp ? 1 : 0;
+          chunk_st += (min(nzm, nw) << 6) + (sp ? 1u : 0u);
         }
         if (lane == j) new_z = k;
         __syncwarp();
+      }
+      if (lane == 0) {
+        atomicAdd(blk_stats + 2, (unsigned long long)(chunk_st >> 6));
+        atomicAdd(blk_stats + 3, (unsigned long long)(chunk_st & 63u));
       }
       if (valid) {
         p.z[off + i] = new_z;
@@ -157,29 +172,32 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
         ll_acc = ll_skip = 0.0;
       }
     }
-    st_tok += L;
-    st_docs += 1;
+    if (lane == 0) {
+      atomicAdd(blk_stats + 0, (unsigned long long)L);
+      atomicAdd(blk_stats + 1, 1ull);
+    }
     __syncwarp();
   }
   if (want_ll && !BATCH) {
     ll_acc = warp_sum_f64(ll_acc);
     ll_skip = warp_sum_f64(ll_skip);
   }
-  if (lane == 0) {
-    atomicAdd(p.counters + kCtrTokens, (unsigned long long)st_tok);
-    atomicAdd(p.counters + kCtrDocs, (unsigned long long)st_docs);
-    atomicAdd(p.counters + kCtrSparseWork, (unsigned long long)st_S);
-    atomicAdd(p.counters + kCtrSparseDraws, (unsigned long long)st_sp);
-    if (want_ll && !BATCH) {
-      atomicAdd(p.ll, ll_acc);
-      atomicAdd(p.ll + 1, ll_skip);
-    }
+  if (lane == 0 && want_ll && !BATCH) {
+    atomicAdd(p.ll, ll_acc);
+    atomicAdd(p.ll + 1, ll_skip);
   }
   status = __reduce_or_sync(kFullMask, status);
   if (lane == 0 && status) atomicOr(p.status, status);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicAdd(p.counters + kCtrTokens, blk_stats[0]);
+    atomicAdd(p.counters + kCtrDocs, blk_stats[1]);
+    atomicAdd(p.counters + kCtrSparseWork, blk_stats[2]);
+    atomicAdd(p.counters + kCtrSparseDraws, blk_stats[3]);
+  }
 }
 
-template <bool BATCH>
+template <bool BATCH, bool LL>
 void launch_impl(const ZKernelArgs& a, u32 n_docs, cudaStream_t s, u32 wpb, u32 blocks_per_sm) {
   const size_t per_warp = doc_counts_bytes(a.Kmax) + kTokStageBytes;
   // Warps per block: as many as fit the shared-memory budget (at most the request).
@@ -188,15 +206,15 @@ void launch_impl(const ZKernelArgs& a, u32 n_docs, cudaStream_t s, u32 wpb, u32 
   // The ceiling, not this launch's size: captured graphs may hold launches of
   // several sizes.
   if (smem > 48 * 1024)
-    cudaFuncSetAttribute(z_sweep_kernel<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZMaxSmem);
+    cudaFuncSetAttribute(z_sweep_kernel<BATCH, LL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZMaxSmem);
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, z_sweep_kernel<BATCH>, 32 * wpb, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, z_sweep_kernel<BATCH, LL>, 32 * wpb, smem);
   if (per_sm < 1) per_sm = 1;
   if (blocks_per_sm && (int)blocks_per_sm < per_sm) per_sm = (int)blocks_per_sm;
   u32 blocks = (u32)(device_sm_count() * per_sm);
   const u32 need = (n_docs + wpb - 1) / wpb;
   if (blocks > need) blocks = need;
-  z_sweep_kernel<BATCH><<<blocks, 32 * wpb, smem, s>>>(a);
+  z_sweep_kernel<BATCH, LL><<<blocks, 32 * wpb, smem, s>>>(a);
 }
 
 }  // namespace
@@ -212,7 +230,10 @@ void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s) {
   a.Kmax = m.K;
   a.lg_a = std::lgamma((double)m.alpha);
   a.lg_Ka = std::lgamma((double)m.K * (double)m.alpha);
-  launch_impl<false>(a, z.n_docs, s, 8, 0);
+  if ((z.flags & 1u) && z.ll)
+    launch_impl<false, true>(a, z.n_docs, s, 8, 0);
+  else
+    launch_impl<false, false>(a, z.n_docs, s, 8, 0);
 }
 
 void launch_z_sweep_batch(const ModelDev& arenas, const BatchDev& b, u32 Kmax, const ZLaunch& z, cudaStream_t s,
@@ -225,7 +246,10 @@ void launch_z_sweep_batch(const ModelDev& arenas, const BatchDev& b, u32 Kmax, c
   a.Kmax = Kmax;
   a.lg_a = 0;
   a.lg_Ka = 0;
-  launch_impl<true>(a, z.n_docs, s, warps_per_block, blocks_per_sm);
+  if ((z.flags & 1u) && z.ll)
+    launch_impl<true, true>(a, z.n_docs, s, warps_per_block, blocks_per_sm);
+  else
+    launch_impl<true, false>(a, z.n_docs, s, warps_per_block, blocks_per_sm);
 }
 
 }  // namespace gpulda
