@@ -6,8 +6,8 @@
 // The list is the order-preserving map of zsweep_map.cu without empty slots:
 // entries (topic << 16 | count), ascending topic.  A topic whose count falls
 // to zero stays as a dead entry (zero mass, so it never changes B or the
-// selected topic) and is revived if the topic returns; more than 32 dead
-// entries are compacted away.  Lookups are warp-cooperative 32-ary searches
+// selected topic) and is revived if the topic returns; more than kPairsMaxDead
+// dead entries are compacted away.  Lookups are warp-cooperative 32-ary searches
 // (two ballot rounds for lists up to 1024 entries); inserts shift the tail.
 // The walk reads the entries in ascending topic order, so the sparse draw is
 // identical to the dense-count kernel's, the map kernel's and the CPU
@@ -20,14 +20,22 @@
 // list; chunks of at most 4 elements keep their masses in registers, so the
 // sparse selection needs no second pass.
 //
-// Capacity per warp: min(lmax, K) live entries, at most 33 dead ones before a
-// compaction, rounded up: min(lmax, K) + 64.  An insert that would pass it is
+// Capacity per warp: min(lmax, K) live entries, at most kPairsMaxDead + 1
+// dead ones before a compaction, rounded up: min(lmax, K) + 64.  An insert that would pass it is
 // refused and reported (it cannot happen under that bound).
 #include <algorithm>
 #include <cmath>
 
 #include "kernels.cuh"
 #include "warp.cuh"
+
+namespace {
+// Dead entries tolerated before a compaction: each costs every walk of the
+// document's entries one zero-mass element, a compaction one pass.  At
+// K=10000 (D = 2e6) 8 gave 129 ms per sweep against 133 ms for 16 and 141 ms
+// for 32.
+constexpr unsigned kPairsMaxDead = 8;
+}  // namespace
 
 namespace gpulda {
 
@@ -127,10 +135,19 @@ __device__ __forceinline__ void pairs_add_at(u32* P, u32& nl, u32& nz, u32 pos, 
   ++nz;
 }
 
-// Three blocks per SM (up to 85 registers, no spills): 1.5x faster at K=10000
-// than four blocks at 64 registers with spills.
-__global__ void __launch_bounds__(256, 3) z_sweep_pairs_kernel(PairArgs a) {
+// Four blocks per SM at 64 registers, with no spills because the joint
+// log-likelihood is a separate instantiation (LL: the plain sweep keeps no
+// log-likelihood registers) and the statistics are per-chunk sums in one
+// register flushed to per-block shared counters.  At K=10000 (D = 2e6): 117.6 ms
+// per sweep, against 129.3 ms at three blocks per SM (68 registers); with the
+// statistics in per-thread u64 counters four blocks spilled and ran 1.5x slower
+// than three.
+template <bool LL>
+__global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
   extern __shared__ __align__(16) unsigned char zsm[];
+  __shared__ unsigned long long blk_stats[4];  // tokens, documents, sparse work, sparse draws
+  if (threadIdx.x < 4) blk_stats[threadIdx.x] = 0;
+  __syncthreads();
   const ModelDev& m = a.m;
   const ZLaunch& p = a.z;
   const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -138,9 +155,8 @@ __global__ void __launch_bounds__(256, 3) z_sweep_pairs_kernel(PairArgs a) {
   unsigned char* wsm = zsm + (size_t)warp * ((size_t)a.cap * 4 + kTokStageBytes);
   u32* P = (u32*)wsm;
   uint4* stage = (uint4*)(wsm + (size_t)a.cap * 4);
-  const bool want_ll = (p.flags & 1u) && p.ll;
+  const bool want_ll = LL;
 
-  u64 st_tok = 0, st_docs = 0, st_S = 0, st_sp = 0;
   double ll_acc = 0.0, ll_skip = 0.0;
   u32 status = 0;
 
@@ -189,6 +205,9 @@ __global__ void __launch_bounds__(256, 3) z_sweep_pairs_kernel(PairArgs a) {
       const u64 my_al = (valid && my_nw) ? __ldg(m.al + my_row + my_s) : 0ull;
       u32 new_z = my_z;
       const u32 nt = min(32u, L - base);
+      // sum over the chunk of (min(nz without the token, nnz[w]) << 6) + sparse
+      // (the first term at most 32 * 32768, the second at most 32)
+      u32 chunk_st = 0;
       __syncwarp();
       stage[2 * lane] = make_uint4(my_z, r.x, r.y, my_nw);
       stage[2 * lane + 1] = make_uint4((u32)my_row, (u32)(my_row >> 32), (u32)my_A, (u32)(my_A >> 32));
@@ -316,14 +335,17 @@ __global__ void __launch_bounds__(256, 3) z_sweep_pairs_kernel(PairArgs a) {
         const u32 nzm = nz;
         if (pos == 0xffffffffu) pos = pairs_lower_bound(P, nl, k, lane);
         pairs_add_at(P, nl, nz, pos, k, a.cap, lane, &status);
-        if (nl - nz > 32u) nl = pairs_compact(P, nl, lane);
+        if (nl - nz > kPairsMaxDead) nl = pairs_compact(P, nl, lane);
         if (lane == 0) {
           atomicAdd(m.n + row + k, 1u);
-          st_S += min(nzm, nw);
-          st_sp += (sp && !degenerate) ? 1 : 0;
+          chunk_st += (min(nzm, nw) << 6) + ((sp && !degenerate) ? 1u : 0u);
         }
         if (lane == j) new_z = k;
         __syncwarp();
+      }
+      if (lane == 0) {
+        atomicAdd(blk_stats + 2, (unsigned long long)(chunk_st >> 6));
+        atomicAdd(blk_stats + 3, (unsigned long long)(chunk_st & 63u));
       }
       if (valid) {
         p.z[off + i] = new_z;
@@ -346,26 +368,29 @@ __global__ void __launch_bounds__(256, 3) z_sweep_pairs_kernel(PairArgs a) {
       dl = warp_sum_f64(dl);
       if (lane == 0) ll_acc += dl + a.lg_Ka - lgamma((double)K * (double)m.alpha + (double)L);
     }
-    st_tok += L;
-    st_docs += 1;
+    if (lane == 0) {
+      atomicAdd(blk_stats + 0, (unsigned long long)L);
+      atomicAdd(blk_stats + 1, 1ull);
+    }
     __syncwarp();
   }
   if (want_ll) {
     ll_acc = warp_sum_f64(ll_acc);
     ll_skip = warp_sum_f64(ll_skip);
   }
-  if (lane == 0) {
-    atomicAdd(p.counters + kCtrTokens, (unsigned long long)st_tok);
-    atomicAdd(p.counters + kCtrDocs, (unsigned long long)st_docs);
-    atomicAdd(p.counters + kCtrSparseWork, (unsigned long long)st_S);
-    atomicAdd(p.counters + kCtrSparseDraws, (unsigned long long)st_sp);
-    if (want_ll) {
-      atomicAdd(p.ll, ll_acc);
-      atomicAdd(p.ll + 1, ll_skip);
-    }
+  if (lane == 0 && want_ll) {
+    atomicAdd(p.ll, ll_acc);
+    atomicAdd(p.ll + 1, ll_skip);
   }
   status = __reduce_or_sync(kFullMask, status);
   if (lane == 0 && status) atomicOr(p.status, status);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicAdd(p.counters + kCtrTokens, blk_stats[0]);
+    atomicAdd(p.counters + kCtrDocs, blk_stats[1]);
+    atomicAdd(p.counters + kCtrSparseWork, blk_stats[2]);
+    atomicAdd(p.counters + kCtrSparseDraws, blk_stats[3]);
+  }
 }
 
 }  // namespace
@@ -387,15 +412,15 @@ bool launch_z_sweep_pairs(const ModelDev& m, const ZLaunch& z, cudaStream_t s, u
   while (wpb > 1 && per_warp * wpb > kBudget) --wpb;
   if (per_warp * wpb > kBudget) return false;
   const size_t smem = per_warp * wpb;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(z_sweep_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBudget);
+  auto kern = ((z.flags & 1u) && z.ll) ? z_sweep_pairs_kernel<true> : z_sweep_pairs_kernel<false>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBudget);
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, z_sweep_pairs_kernel, 32 * wpb, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, smem);
   if (per_sm < 1) per_sm = 1;
   u32 blocks = (u32)(device_sm_count() * per_sm);
   const u32 need = (z.n_docs + wpb - 1) / wpb;
   if (blocks > need) blocks = need;
-  z_sweep_pairs_kernel<<<blocks, 32 * wpb, smem, s>>>(a);
+  kern<<<blocks, 32 * wpb, smem, s>>>(a);
   return true;
 }
 
