@@ -33,9 +33,9 @@ namespace gpulda {
 // Dead list entries (topics whose count fell to zero) tolerated before the
 // list is compacted.  Each costs every walk of the document's list one
 // zero-mass element; a compaction costs a pass over the list.  Measured on the
-// mid corpus (K=1000), fifth iteration: 0 -> 37.2 ms per sweep, 8 -> 36.8,
-// 16 -> 37.2, 32 -> 38.2, 64 -> 39.3.
-constexpr u32 kMaxDead = 8;
+// mid corpus (K=1000), fifth iteration: 0 -> 37.2 ms per sweep, 4 -> 36.6,
+// 8 -> 36.8, 16 -> 37.2, 32 -> 38.2, 64 -> 39.3.
+constexpr u32 kMaxDead = 4;
 
 // Shared memory per warp for documents of up to Kmax topics: counts and list
 // (2 x Kp u16) and the in-list bitmap.
@@ -154,6 +154,12 @@ __device__ __forceinline__ void doc_counts_build(DocCounts& dc, const u32* z, u3
 // the word's fixed-point Phi row and nonzero list, nw its list length, Aw its
 // dense mass.  Returns the topic; *nz_minus receives the document's distinct
 // topics without the token, *sparse whether the sparse branch chose it.
+// kRegChunk: the longest per-lane chunk kept in registers (lists up to 32 x
+// kRegChunk entries need no second pass); 6 for the single-model sweep (mid
+// corpus: 4 -> 36.8 ms, 6 -> 36.3, 8 -> 42.1 with spills), 4 where the caller
+// holds more registers of its own (the batched sweep and the fold-in spill at
+// 6).
+template <u32 kRegChunk = 6>
 __device__ __forceinline__ u32 token_step(DocCounts& dc, u32 zj, u32 r0, u32 r1, u32 my_r3, u64 my_al, u32 j,
                                           const u32* __restrict__ qrow, const u64* __restrict__ crow, u32 nw, u64 Aw,
                                           float alpha, u32 lane, u32* nz_minus, bool* sparse) {
@@ -171,10 +177,9 @@ __device__ __forceinline__ u32 token_step(DocCounts& dc, u32 zj, u32 r0, u32 r1,
   const u32 len = word_side ? nw : nl;
   const u32 cper = (len + 31) >> 5;
   const u32 e0 = min(len, lane * cper), e1 = min(len, e0 + cper);
-  // Chunks of at most 4 elements (lists up to 128 entries): unrolled
+  // Chunks of at most kRegChunk elements (lists up to 32 kRegChunk entries): unrolled
   // independent loads, masses kept in registers, so the selection needs no
   // second pass; the crossing element's topic is read once afterwards.
-  constexpr u32 kRegChunk = 4;
   const bool in_regs = cper <= kRegChunk;
   u64 ms[kRegChunk];
   u64 ls = 0;

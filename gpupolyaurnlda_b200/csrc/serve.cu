@@ -158,7 +158,7 @@ __device__ void fold_request(const FoldCommon& a, DocCounts& dc, uint4* stage, c
         const u64 Aw = ((u64)s1.w << 32) | s1.z;
         u32 nzm;
         bool sp;
-        const u32 k = token_step(dc, zj, r0, r1, r.w, my_al, j, m.q + row, m.csr + row, nw, Aw, alpha, lane, &nzm,
+        const u32 k = token_step<4u>(dc, zj, r0, r1, r.w, my_al, j, m.q + row, m.csr + row, nw, Aw, alpha, lane, &nzm,
                                  &sp);
         if (lane == j) new_z = k;
         __syncwarp();

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(256, 4) z_sweep_kernel(ZKernelArgs a) {
         const u64 Aw = ((u64)s1.w << 32) | s1.z;
         u32 nzm;
         bool sp;
-        const u32 k = token_step(dc, zj, r0, r1, r.w, my_al, j, m.q + row, m.csr + row, nw, Aw, alpha, lane, &nzm,
+        const u32 k = token_step<BATCH ? 4u : 6u>(dc, zj, r0, r1, r.w, my_al, j, m.q + row, m.csr + row, nw, Aw, alpha, lane, &nzm,
                                  &sp);
         if (lane == 0) {
           atomicAdd(m.n + row + k, 1u);
