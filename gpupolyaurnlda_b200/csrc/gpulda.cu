@@ -35,6 +35,11 @@ enum TimerSlot { kTPhi = 0, kTPrep = 1, kTAlias = 2, kTOffsets = 3, kTZ = 4, kTN
 // A buffer's sweep is split into this many pieces of about equal token counts
 // so that copying piece p+1 in and piece p-1 out overlaps sweeping piece p.
 constexpr u32 kPieces = 8;
+// Piece p ends at kPieceEnd[p] / 32 of the buffer's tokens.  The first piece
+// is small because its copy in is the one wait the sweep cannot hide, the last
+// because its copy out is the one that follows the whole sweep; the copies
+// (about 55 GB/s each way) outrun the sweep in between.
+constexpr u32 kPieceEnd[kPieces] = {1, 3, 7, 12, 18, 24, 29, 32};
 // A piece's documents of at least this many times its mean length are swept by
 // a separate launch on a high-priority stream: the block scheduler then starts
 // them as soon as their piece has arrived and a block slot frees, instead of
@@ -446,7 +451,7 @@ int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_
 }
 
 // sample_z_async for host buffers: kPieces pieces of whole documents with
-// about equal token counts; piece p's tokens are copied in on the h2d stream,
+// token counts in the proportions of kPieceEnd; piece p's tokens are copied in on the h2d stream,
 // swept on the buffer's stream once they have arrived, and copied out on the
 // d2h stream once swept.  Token numbering stays buffer-relative, so the result
 // does not depend on the split.
@@ -462,7 +467,7 @@ int pipelined_sweep(Buffer* b, BufCtx* ctx) {
   u32 pc = 1;
   for (u32 i = 0; i < n && pc < kPieces; ++i) {
     cum += b->d[i];
-    while (pc < kPieces && cum * kPieces >= (u64)b->n_tokens * pc) {
+    while (pc < kPieces && cum * 32 >= (u64)b->n_tokens * kPieceEnd[pc - 1]) {
       dcut[pc] = i + 1;
       tcut[pc] = std::min<u64>(cum, b->n_tokens);
       ++pc;
