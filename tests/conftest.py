@@ -23,8 +23,9 @@ def oracle_lib():
 
 @pytest.fixture(scope="session")
 def small_corpus():
-    """The small workload (K=20, V~5000, D=2000, ~200k tokens), regenerated
-    from its seed and checked against the committed fixture's digest."""
+    """The small workload (K=20, V~3300, D=2000, ~200k tokens), regenerated
+    from its seed; tests/test_golden.py checks it against the committed
+    fixture's digests (tests/golden/small_chain.json)."""
     from gpupolyaurnlda_b200 import corpus
     return corpus.generate("small", seed=1)
 

@@ -126,6 +126,34 @@ def test_small_chain_parity(gpu_lib, oracle_lib, small_corpus):
     assert (z_gpu != c.z).mean() > 0.5
 
 
+def test_small_chain_golden(gpu_lib, small_corpus):
+    """Five iterations of the small workload through the reference protocol
+    against the committed golden fixture (digests of the oracle's topics and
+    counts after every iteration): no oracle runs beside it."""
+    import hashlib
+    import json
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "small_chain.json")) as f:
+        golden = json.load(f)
+    c = small_corpus
+    z = c.z.astype(np.uint32).copy()
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+    with g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=c.n_tokens, max_D=c.n_docs,
+                   seed=golden["sampler_seed"], flags=g.GPULDA_FLAG_LOGLIK) as s:
+        for w in golden["iterations"]:
+            s.sample_phi()
+            s.sweep_buffer(0, z, c.w, c.d_len, c.k_d())
+            n = s.read_state(q=False, alias=False, A=False, S=False, nnz=False)["n"]
+            assert z[:64].tolist() == w["z_first_64"], w["t"]
+            assert sha(z) == w["sha256_z"], w["t"]
+            assert sha(n.astype(np.uint32)) == w["sha256_n"], w["t"]
+            ll, skipped = s.loglik()
+            assert abs(ll - w["ll"]) <= LL_RTOL * abs(w["ll"]) and skipped == w["ll_skipped"], (w["t"], ll)
+            cnt = s.counters()
+            assert cnt["sparse_work"] == w["sparse_work"] and cnt["sparse_draws"] == w["sparse_draws"], w["t"]
+
+
 def test_buffers_and_corpus_mode_agree(gpu_lib, oracle_lib, small_corpus):
     """Splitting the corpus into buffers (max_D = 300 documents, as the
     reference's fill_buffer does) or keeping it resident gives the same chain."""
