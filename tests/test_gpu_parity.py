@@ -181,6 +181,35 @@ def test_buffers_and_corpus_mode_agree(gpu_lib, oracle_lib, small_corpus):
     assert (z_buf == z_orc).all()
 
 
+def test_buffer_lengths_rewritten_in_place(gpu_lib, oracle_lib, small_corpus):
+    """The host-buffer sweep reuses its pieces and document order while the
+    lengths array is unchanged; rewriting the same arrays in place between
+    iterations (documents in reverse order: same counts and totals) must be
+    noticed, and the chain must still equal the oracle's."""
+    c = small_corpus
+    d = c.d_len.astype(np.uint32).copy()
+    w = c.w.astype(np.uint32).copy()
+    kd = c.k_d().astype(np.uint32).copy()
+    z_gpu = c.z.astype(np.uint32).copy()
+    z_orc = z_gpu.copy()
+    ch = oracle_lib.Chain(c.K, c.alpha, c.beta, c.counts, seed=5)
+    with g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=c.n_tokens, max_D=c.n_docs, seed=5) as s:
+        for it in range(5):
+            if it in (2, 4):
+                offs = np.concatenate([[0], np.cumsum(d.astype(np.int64))])
+                perm = np.concatenate([np.arange(offs[i], offs[i + 1]) for i in range(len(d) - 1, -1, -1)])
+                d[:] = d[::-1].copy()
+                kd[:] = kd[::-1].copy()
+                w[:] = w[perm]
+                z_gpu[:] = z_gpu[perm]
+                z_orc[:] = z_orc[perm]
+            s.sample_phi()
+            ch.sample_phi()
+            s.sweep_buffer(0, z_gpu, w, d, kd)
+            ch.sweep(w, z_orc, d)
+            assert (z_gpu == z_orc).all(), f"iteration {it}: {(z_gpu != z_orc).sum()} topics differ"
+
+
 def test_sample_topics_concentrated(gpu_lib):
     """src/cu/test/test_topics.cu:276-334 restated: Phi concentrated on topic 0
     (beta = 0, counts only in topic 0) sends every token to topic 0."""
