@@ -123,7 +123,6 @@ void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s);
 // warps per block and cap on blocks per SM (0: as many as fit).
 void launch_z_sweep_batch(const ModelDev& arenas, const BatchDev& b, u32 Kmax, const ZLaunch& z, cudaStream_t s,
                           u32 warps_per_block, u32 blocks_per_sm);
-size_t z_sweep_smem_per_warp(u32 K);
 // The same sweep with each document's counts in a shared-memory hash map
 // (large K).  Documents longer than lmax are reported, not swept.  Returns
 // false without launching when lmax needs more shared memory than a block has.

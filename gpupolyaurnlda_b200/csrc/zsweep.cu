@@ -219,8 +219,6 @@ void launch_impl(const ZKernelArgs& a, u32 n_docs, cudaStream_t s, u32 wpb, u32 
 
 }  // namespace
 
-size_t z_sweep_smem_per_warp(u32 K) { return doc_counts_bytes(K) + kTokStageBytes; }
-
 void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s) {
   if (!z.n_docs) return;
   ZKernelArgs a;
