@@ -114,3 +114,38 @@ def test_loglik_improves(oracle_lib, small_corpus):
         ch.sample_phi()
         lls.append(ch.sweep(c.w, z, c.d_len, want_ll=True)["ll"])
     assert lls[-1] > lls[0] + 0.1 * abs(lls[0])
+
+
+def test_fold_in_properties(oracle_lib, small_corpus):
+    """Fold-in of new documents against a fixed model (the serving path's
+    definition): theta is a distribution with the (m + alpha) / (L + K alpha)
+    form, a result depends only on its request id and words (not on the other
+    requests of the call, their order or the thread count), and different ids
+    draw differently."""
+    c = small_corpus
+    ch = oracle_lib.Chain(c.K, c.alpha, c.beta, c.counts, seed=2)
+    ch.sample_phi()
+    ch.sweep(c.w, c.z.astype(np.uint32).copy(), c.d_len)
+    ch.sample_phi()
+    phi = ch.phi
+    rng = np.random.default_rng(0)
+    lengths = rng.integers(5, 200, 12).astype(np.uint32)
+    words = rng.integers(0, c.V, int(lengths.sum())).astype(np.uint32)
+    ids = np.arange(100, 112, dtype=np.uint64)
+    r = oracle_lib.fold_in(c.K, c.V, c.alpha, phi, words, lengths, ids, 20, seed=2)
+    assert np.allclose(r["theta"].sum(axis=1), 1.0, atol=1e-5)
+    m = np.rint((r["theta"].astype(np.float64) * (lengths[:, None] + c.K * c.alpha)) - c.alpha)
+    assert (m.sum(axis=1) == lengths).all() and (m >= 0).all()
+    assert np.isfinite(r["ll"]).all() and (r["ll"] < 0).all()
+    # each request alone, in reverse order, and with one thread
+    offs = np.concatenate([[0], np.cumsum(lengths.astype(np.int64))])
+    for i in (0, 5, 11):
+        one = oracle_lib.fold_in(c.K, c.V, c.alpha, phi, words[offs[i]:offs[i + 1]], lengths[i:i + 1], ids[i:i + 1],
+                                 20, seed=2, threads=1)
+        assert (one["theta"][0] == r["theta"][i]).all() and one["ll"][0] == r["ll"][i]
+    rev = oracle_lib.fold_in(c.K, c.V, c.alpha, phi,
+                             np.concatenate([words[offs[i]:offs[i + 1]] for i in range(11, -1, -1)]),
+                             lengths[::-1].copy(), ids[::-1].copy(), 20, seed=2)
+    assert (rev["theta"][::-1] == r["theta"]).all()
+    other = oracle_lib.fold_in(c.K, c.V, c.alpha, phi, words, lengths, ids + np.uint64(1000), 20, seed=2)
+    assert (other["theta"] != r["theta"]).any()
