@@ -37,7 +37,7 @@ def _stale(target: str, deps: list[str]) -> bool:
 
 def _deps() -> list[str]:
     out = []
-    for d in (CSRC, os.path.join(ROOT, "include")):
+    for d in (CSRC, os.path.join(CSRC, "host"), os.path.join(ROOT, "include")):
         for f in os.listdir(d):
             if f.endswith((".cu", ".cuh", ".h", ".cpp")):
                 out.append(os.path.join(d, f))

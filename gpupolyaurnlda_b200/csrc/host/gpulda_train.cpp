@@ -359,9 +359,37 @@ void output(const Options& o) {
   unmap(md);
 }
 
+// The flags of src/args.rs:16-61 with their defaults, plus this twin's own.
+void usage(FILE* f) {
+  const Options d;
+  fprintf(f,
+          "gpulda_train: preprocess, train and output as the reference's command line does\n"
+          "  --alpha F          alpha parameter (%g)\n"
+          "  --beta F           beta parameter (%g)\n"
+          "  --K N              number of topics (%u)\n"
+          "  --buffer_size N    tokens per buffer (%u)\n"
+          "  --max_D N          documents per buffer (%u)\n"
+          "  --n_mc N           Gibbs iterations (%u)\n"
+          "  --seed N           random number seed (%u)\n"
+          "  --input PATH       corpus text (%s)\n"
+          "  --output PATH      token:topic output (%s)\n"
+          "  --z_temp_file, --w_temp_file, --d_temp_file, --K_d_temp_file PATH   u32 binaries (%s, %s, %s, %s)\n"
+          "  --c_temp_file PATH word counts, one per line (%s)\n"
+          "  --phases LIST      comma-separated subset of preprocess,train,output (%s)\n"
+          "  --double_buffer 0|1  two buffers in flight (%d)\n"
+          "  --pin 0|1          page-lock the mapped files (%d)\n",
+          d.alpha, d.beta, d.K, d.buffer_size, d.max_D, d.n_mc, d.seed, d.input.c_str(), d.output.c_str(),
+          d.z.c_str(), d.w.c_str(), d.d.c_str(), d.k_d.c_str(), d.c.c_str(), d.phases.c_str(), (int)d.double_buffer,
+          (int)d.pin);
+}
+
 bool parse(int argc, char** argv, Options& o) {
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
+    if (a == "--help" || a == "-h") {
+      usage(stdout);
+      exit(0);
+    }
     auto val = [&](void) -> std::string {
       if (i + 1 >= argc) {
         fprintf(stderr, "missing value for %s\n", a.c_str());
@@ -388,6 +416,7 @@ bool parse(int argc, char** argv, Options& o) {
     else if (a == "--pin") o.pin = std::stoul(val()) != 0;
     else {
       fprintf(stderr, "unknown flag %s\n", a.c_str());
+      usage(stderr);
       return false;
     }
   }

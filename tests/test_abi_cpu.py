@@ -134,6 +134,15 @@ def test_gpulda_train_binary_parses_reference_flags(built):
     assert os.path.exists(exe)
     r = subprocess.run([exe, "--no_such_flag"], capture_output=True, text=True)
     assert r.returncode == 2 and "unknown flag" in r.stderr
+    # --help lists every flag of src/args.rs:16-61 with the reference's defaults
+    r = subprocess.run([exe, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0
+    for flag, default in [("--alpha", "0.1"), ("--beta", "0.1"), ("--K", "100"), ("--buffer_size", "33554432"),
+                          ("--max_D", "16384"), ("--n_mc", "1"), ("--seed", "0"), ("--input", "data/small.txt"),
+                          ("--output", "output/small.txt"), ("--z_temp_file", "temp/z.bin"),
+                          ("--w_temp_file", "temp/w.bin"), ("--d_temp_file", "temp/d.bin"),
+                          ("--K_d_temp_file", "temp/k_d.bin"), ("--c_temp_file", "temp/c.txt")]:
+        assert flag in r.stdout and default in r.stdout, flag
 
 
 def test_batch_problem_layout():
