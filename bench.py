@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="mid")
     p.add_argument("--docs", type=int, default=None, help="override the number of documents")
+    p.add_argument("--vocab", type=int, default=None,
+                   help="override the vocabulary size (small profiling cases of the large-K workloads)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
@@ -180,8 +182,12 @@ def roofline_profile(workload: str, c) -> dict:
 
 
 def make_corpus(args, device):
+    import dataclasses
     from gpupolyaurnlda_b200 import corpus
-    return corpus.generate(args.workload, seed=1, device=device, D=args.docs)
+    wl = corpus.WORKLOADS[args.workload]
+    if getattr(args, "vocab", None):
+        wl = dataclasses.replace(wl, V=args.vocab)
+    return corpus.generate(wl, seed=1, device=device, D=args.docs)
 
 
 def workload_desc(c, args):
