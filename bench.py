@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
+    p.add_argument("--no-large", action="store_true", help="skip the large-K summary of the default line")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-chains summary of the default line")
+    p.add_argument("--large-steps", type=int, default=3, help="large-K summary: timed iterations")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU seconds per timed oracle iteration")
     p.add_argument("--problems", type=int, default=64, help="batched workload: number of problems")
     p.add_argument("--batch-scale", type=float, default=1.0, help="batched workload: scale of each problem's D")
@@ -206,6 +209,7 @@ class CpuChain:
 
     def __init__(self, c, seconds: float, threads: int | None = None):
         import oracle
+        self.lib_path = oracle_native(oracle)
         self.c = c
         self.threads = threads or oracle.default_threads()
         self.ch = oracle.Chain(c.K, c.alpha, c.beta, c.counts, seed=0, threads=self.threads)
@@ -238,11 +242,19 @@ class CpuChain:
 
     def describe(self, value: float, warm: int) -> dict:
         t_phi, t_z = self.last
-        return {"value": value, "unit": UNIT, "cores": self.threads, "kind": "port",
+        return {"value": value, "unit": UNIT, "cores": self.threads, "kind": "port", "build": self.lib_path,
                 "sample": f"CPU oracle chain on the first {self.docs} documents ({self.ntok} of {self.c.n_tokens} "
                           f"tokens) after {warm} warm-up iterations; per iteration a Phi step over all "
                           f"{self.c.K}x{self.c.V} cells ({t_phi:.2f} s) and a z sweep of the slice ({t_z:.2f} s), "
                           f"extrapolated to the whole corpus"}
+
+
+def oracle_native(oracle) -> str:
+    """The timed CPU legs run the oracle built with -march=native on this host
+    (oracle/build.py; same results bit for bit as the portable build)."""
+    if oracle._lib is None:
+        oracle.use_native_build()
+    return os.path.basename(oracle._path)
 
 
 def cpu_baseline(c, seconds: float, warm: int = 2):
@@ -270,7 +282,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
-            "config": dict(workload_desc(c, args), parallelism="cpu"),
+            "config": workload_desc(c, args), "parallelism": f"CPU, {cc.threads} threads",
             "cpu_baseline": cc.describe(v, args.warmup),
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "CPU oracle port of the sweep (the reference has no CPU implementation of the path; its CUDA "
@@ -345,8 +357,9 @@ def run_ours(args):
         from gpupolyaurnlda_b200.serve import Server
         srv_b = Server(50, seed=0, max_inflight=1 << 17)
         srv_u = Server(50, mode="launch", slots=args.serve_slots, max_batch=1, seed=0)
+        q_model = s.read_state(n=False, alias=False, A=False, S=False, nnz=False)["q"]
         s.close()
-        rows, ll = serve_measure(srv_b, srv_u, [1000, 50000], 2.0, 100000, 3000, local)
+        rows, ll = serve_measure(srv_b, srv_u, q_model, [1000, 10000, 50000], 2.0, 100000, 3000, local)
         srv_b.close()
         srv_u.close()
         serving = {"metric": "served_docs_per_sec", "unit": "docs/s",
@@ -361,35 +374,57 @@ def run_ours(args):
     else:
         s.close()
 
+    large = batched = None
+    if world == 1 and not args.no_large and args.workload == "mid":
+        large = large_k_measure(args, local, hbm)
+    if world == 1 and not args.no_batched and args.workload == "mid":
+        import argparse as _ap
+        bargs = _ap.Namespace(**vars(args))
+        bargs.steps, bargs.warmup = 3, 2
+        r = batched_measure(bargs, local, 1, 0)
+        batched = {k: r[k] for k in ("value", "ms_per_step", "steps", "warmup", "workload", "mode", "sequential",
+                                     "speedup_vs_sequential", "loglik_max_rel_diff_vs_solo", "autotuner", "clocks")}
+        batched["metric"] = "batched_gibbs_tokens_per_sec"
+        torch.cuda.empty_cache()
+
     value = replica_value(c.n_tokens, args.steps, world, ms_max / 1e3)
     zb = [24 * c.n_tokens + 8 * c.n_docs + 4 * S for S in S_work]
     z_gbs = float(np.mean([b / (m / 1e3) / 1e9 for b, m in zip(zb, z_ms)]))
     B_iter = [20 * c.K * c.V + b for b in zb]
     it_gbs = float(np.mean([b / (ms_max / args.steps / 1e3) / 1e9 for b in B_iter]))
 
-    # ---- reference protocol with pinned host buffers: e2e --------------------
-    e2e = None
+    # ---- reference protocol through the C ABI: e2e ---------------------------
+    # Pinned host buffers (gpulda_pin_host exists for callers that can pin),
+    # and pageable ones: the reference's host maps its files pageable
+    # (src/train.rs:77-83), the default path of a caller that does nothing more.
+    e2e = e2e_pageable = None
     if not args.no_e2e:
+        def protocol(zn, wn, dn, kn):
+            s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=c.n_tokens, max_D=c.n_docs, seed=0,
+                          chain=rank)
+            for _ in range(args.warmup):
+                s.sample_phi()
+                s.sweep_buffer(0, zn, wn, dn, kn)
+            if world > 1:
+                dist.barrier()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                s.sample_phi()
+                s.sweep_buffer(0, zn, wn, dn, kn)
+            el = max_over_ranks(time.perf_counter() - t0, f"cuda:{local}")
+            s.close()
+            return {"value": replica_value(c.n_tokens, args.steps, world, el), "unit": UNIT,
+                    "h2d_bytes_per_step": 8 * c.n_tokens + 8 * c.n_docs, "d2h_bytes_per_step": 4 * c.n_tokens}
+
         zp = torch.from_numpy(c.z.copy()).pin_memory()
         wp = torch.from_numpy(c.w).pin_memory()
         dp = torch.from_numpy(c.d_len).pin_memory()
         kp = torch.from_numpy(c.k_d()).pin_memory()
-        zn, wn, dn, kn = zp.numpy(), wp.numpy(), dp.numpy(), kp.numpy()
-        s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=c.n_tokens, max_D=c.n_docs, seed=0, chain=rank)
-        for _ in range(args.warmup):
-            s.sample_phi()
-            s.sweep_buffer(0, zn, wn, dn, kn)
-        if world > 1:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            s.sample_phi()
-            s.sweep_buffer(0, zn, wn, dn, kn)
-        el = max_over_ranks(time.perf_counter() - t0, f"cuda:{local}")
-        s.close()
-        e2e = {"value": replica_value(c.n_tokens, args.steps, world, el), "unit": UNIT,
-               "h2d_bytes_per_step": 8 * c.n_tokens + 8 * c.n_docs, "d2h_bytes_per_step": 4 * c.n_tokens,
-               "path": "initialize/sample_phi/sample_z_async/sync_buffer, one buffer per iteration, pinned host"}
+        e2e = dict(protocol(zp.numpy(), wp.numpy(), dp.numpy(), kp.numpy()),
+                   path="initialize/sample_phi/sample_z_async/sync_buffer, one buffer per iteration, pinned host")
+        del zp, wp, dp, kp
+        e2e_pageable = dict(protocol(c.z.copy(), c.w, c.d_len, c.k_d()),
+                            path="the same protocol with pageable host arrays (no pinning)")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -399,8 +434,8 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-                "config": dict(workload_desc(c, args),
-                               parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+                "config": workload_desc(c, args),
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "roofline": dict({"bound": "hbm", "achieved": z_gbs, "peak": hbm, "unit": "GB/s",
                                   "frac": z_gbs / hbm,
                                   "algorithmic_bytes_per_launch": float(np.mean(zb)), "peak_kind": peak_kind},
@@ -416,10 +451,60 @@ def run_ours(args):
                     "alias_build": (8 * c.K * c.V + 16 * nnz_total) / (float(np.mean(alias_ms)) / 1e3) / 1e9,
                     "z_sweep": z_gbs},
                 "sparse_work_per_token": float(np.mean(S_work)) / c.n_tokens,
-                "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving}
+                "gpu_launches": launches, "clocks": clk, "e2e": e2e, "e2e_pageable": e2e_pageable,
+                "cpu_baseline": cpu, "serving": serving, "large_k10000": large, "batched": batched}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def large_k_measure(args, local: int, hbm: float, workload: str = "large_k10000") -> dict:
+    """The large sweep at K=10000 (V=140,000, D=8,000,000, ~6.4e8 tokens;
+    the sorted-pair-list store) with the corpus resident: 2 warm-up iterations,
+    then `args.large_steps` timed ones (CUDA events on the library's stream).
+    A summary beside the headline, not a second headline."""
+    import torch
+
+    import gpupolyaurnlda_b200 as g
+    from gpupolyaurnlda_b200 import corpus
+    t0 = time.perf_counter()
+    c = corpus.generate(workload, seed=1, device=f"cuda:{local}")
+    t_gen = time.perf_counter() - t0
+    torch.cuda.empty_cache()  # the generator's buffers
+    stream = torch.cuda.Stream()
+    s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=0)
+    s.set_stream(stream.cuda_stream)
+    s.corpus_load(c.z.copy(), c.w, c.d_len)
+    s.corpus_sweep(2)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    z_ms, phi_ms, S_work = [], [], []
+    e0.record(stream)
+    for _ in range(args.large_steps):
+        s.corpus_sweep(1)
+        kt = s.kernel_times()
+        z_ms.append(kt["z_sweep"])
+        phi_ms.append(kt["phi_draw"] + kt["alias_build"] + kt["prep"])
+        S_work.append(s.counters()["sparse_work"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.large_steps
+    s.set_stream(0)
+    s.close()
+    zb = [24 * c.n_tokens + 8 * c.n_docs + 4 * S for S in S_work]
+    z_gbs = float(np.mean([b / (m / 1e3) / 1e9 for b, m in zip(zb, z_ms)]))
+    out = {"workload": f"{workload}: K={c.K} V={c.V} D={c.n_docs} N={c.n_tokens} (synthetic, seed 1), iterations "
+                       f"3..{2 + args.large_steps} of a chain from random topics",
+           "tokens_per_s": c.n_tokens / (ms / 1e3), "ms_per_iteration": ms,
+           "z_sweep_ms": float(np.mean(z_ms)), "phi_step_ms": float(np.mean(phi_ms)),
+           "z_kernel": "z_sweep_pairs_kernel (sorted (topic, count) lists)",
+           "roofline_frac": z_gbs / hbm, "z_achieved_gbs": z_gbs,
+           "sparse_work_per_token": float(np.mean(S_work)) / c.n_tokens, "generate_s": t_gen, "clocks": clk}
+    del c
+    return out
 
 
 def batched_problems(args, device, chain: int):
@@ -434,23 +519,16 @@ def batched_problems(args, device, chain: int):
     return specs
 
 
-def run_batched(args):
-    """Batched chains: all problems in one graph-replayed iteration, against
-    the same problems run one after another as solo models (the same
-    iterations, seeds and chains, so the final log-likelihoods must agree)."""
+def batched_measure(args, local: int, world: int, rank: int) -> dict:
+    """Batched chains: all problems in one graph-replayed iteration (after the
+    autotuner), against the same problems run one after another as solo
+    models (the same iterations, seeds and chains, so the final
+    log-likelihoods must agree).  Returns the measurement."""
     import torch
-    import torch.distributed as dist
 
     import gpupolyaurnlda_b200 as g
     from gpupolyaurnlda_b200.batch import BatchChains
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     t0 = time.perf_counter()
     specs = batched_problems(args, f"cuda:{local}", rank)
     t_gen = time.perf_counter() - t0
@@ -472,6 +550,7 @@ def run_batched(args):
     clocks = ClockSampler(local)
     clocks.start()
     if world > 1:
+        import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
     e0.record(stream)
@@ -505,47 +584,70 @@ def run_batched(args):
     rel = max(abs(a - c) / abs(c) for a, c in zip(ll_b, ll_s))
     value = replica_value(N, args.steps, world, ms_max / 1e3)
     seq_value = replica_value(N, args.steps, world, seq_max / 1e3)
+    Ks = [sp.K for sp in specs]
+    return {"value": value, "ms_per_step": ms_max / args.steps, "steps": args.steps, "warmup": args.warmup,
+            "workload": f"batched: {len(specs)} independent problems, K in {{50,200,1000}} "
+                        f"({Ks.count(50)}/{Ks.count(200)}/{Ks.count(1000)}), V in [5k,50k], "
+                        f"D in [1k,100k] x{args.batch_scale}, doc lengths lognormal(4.5,1.0); "
+                        f"N={N} tokens, D={D} documents",
+            "N": N, "D": D, "cells": info["cells"], "device_bytes": info["device_bytes"],
+            "mode": "merged: one launch per stage over every problem" if info.get("merged") else
+                    "per-bucket concurrent branches",
+            "sequential": {"value": seq_value, "unit": UNIT, "ms_per_step": seq_max / args.steps,
+                           "what": "the same problems one after another as solo models (gpulda_corpus_sweep), "
+                                   "device time summed"},
+            "speedup_vs_sequential": value / seq_value,
+            "loglik_max_rel_diff_vs_solo": rel,
+            "autotuner": {"entries_tuned": n_tuned, "seconds": t_tune,
+                          "shapes": {b_: list(sh) for b_, sh in zip(("K<=64", "K<=256", "K<=1024", "K<=2048"),
+                                                                     shapes) if sh[0]}},
+            "setup_seconds": {"generate": t_gen, "create": t_create},
+            "gpu_launches": args.steps * (1 + (3 if info.get("merged") else 3 * info["buckets"])), "clocks": clk}
+
+
+def run_batched(args):
+    """The batched-chains workload as its own line."""
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    r = batched_measure(args, local, world, rank)
     if rank == 0:
-        Ks = [sp.K for sp in specs]
-        line = {"metric": "batched_gibbs_tokens_per_sec", "value": value, "unit": UNIT, "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        line = {"metric": "batched_gibbs_tokens_per_sec", "value": r["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
                 "data": "synthetic",
-                "config": {"workload": f"batched: {len(specs)} independent problems, K in {{50,200,1000}} "
-                                       f"({Ks.count(50)}/{Ks.count(200)}/{Ks.count(1000)}), V in [5k,50k], "
-                                       f"D in [1k,100k] x{args.batch_scale}, doc lengths lognormal(4.5,1.0); "
-                                       f"N={N} tokens, D={D} documents",
-                           "N": N, "D": D, "cells": info["cells"], "device_bytes": info["device_bytes"],
-                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                           "l2": "inputs larger than L2"},
-                "sequential": {"value": seq_value, "unit": UNIT, "ms_per_step": seq_max / args.steps,
-                               "what": "the same problems one after another as solo models (gpulda_corpus_sweep), "
-                                       "device time summed"},
-                "speedup_vs_sequential": value / seq_value,
-                "loglik_max_rel_diff_vs_solo": rel,
-                "autotuner": {"buckets_tuned": n_tuned, "seconds": t_tune,
-                              "shapes": {b_: list(sh) for b_, sh in zip(("K<=64", "K<=256", "K<=1024", "K<=2048"),
-                                                                         shapes) if sh[0]}},
-                "setup_seconds": {"generate": t_gen, "create": t_create},
-                "gpu_launches": args.steps * (1 + 3 * info["buckets"]), "clocks": clk}
+                "config": {"workload": r["workload"], "N": r["N"], "D": r["D"], "cells": r["cells"],
+                           "device_bytes": r["device_bytes"], "l2": "inputs larger than L2"},
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+        line.update({k: r[k] for k in ("mode", "sequential", "speedup_vs_sequential", "loglik_max_rel_diff_vs_solo",
+                                       "autotuner", "setup_seconds", "gpu_launches", "clocks")})
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
-def serve_open_loop(srv, lengths, words, arrival_s, ids):
+def serve_open_loop(srv, lengths, words, arrival_s, ids, keep_theta: int = 0):
     """Submits requests at their arrival times (open loop), keeps the server
     progressing and collects results.  Returns docs/s (requests over the time
     from the first arrival to the last completion), latencies (ns, completion
-    minus scheduled arrival) and per-request log-likelihoods and skipped
-    counts, in request order."""
+    minus scheduled arrival), per-request log-likelihoods and skipped counts
+    in request order, and the theta rows of the first `keep_theta` requests."""
     n = len(lengths)
+    K = srv.K
     offs = np.concatenate([[0], np.cumsum(lengths.astype(np.int64))])
     t0 = time.monotonic_ns() + 2_000_000
     arr = t0 + (arrival_s * 1e9).astype(np.int64)
     lat = np.zeros(n, np.int64)
     ll = np.zeros(n, np.float64)
     sk = np.zeros(n, np.int64)
+    theta = np.zeros((keep_theta, K), np.float32)
     seen = np.zeros(n, bool)
     i = done = 0
     last = 0
@@ -558,7 +660,7 @@ def serve_open_loop(srv, lengths, words, arrival_s, ids):
             i = j
             busy = True
         srv.progress()
-        out = srv.poll(1 << 16, theta=False)
+        out = srv.poll(1 << 14, theta=keep_theta > 0)
         k = len(out["ids"])
         if k:
             r = (out["ids"] - ids[0]).astype(np.int64)
@@ -566,52 +668,69 @@ def serve_open_loop(srv, lengths, words, arrival_s, ids):
             ll[r] = out["ll"]
             sk[r] = out["skipped"]
             seen[r] = True
+            if keep_theta:
+                m = r < keep_theta
+                theta[r[m]] = out["theta"][m]
             last = max(last, int(out["done_ns"].max()))
             done += k
             busy = True
         if not busy:
             time.sleep(2e-5)
     assert seen.all()
-    return n / ((last - arr[0]) / 1e9), lat, ll, sk
+    return n / ((last - arr[0]) / 1e9), lat, ll, sk, theta
 
 
-def serve_measure(srv_b, srv_u, rates, seconds, max_requests, max_unbatched, local):
+def serve_measure(srv_b, srv_u, q, rates, seconds, max_requests, max_unbatched, local):
     """Open-loop serving runs at the given offered rates against the batched
-    (persistent) and the one-launch-per-document servers; returns the per-rate
-    rows and the held-out log-likelihood per token of both (same requests)."""
-    from gpupolyaurnlda_b200.serve import zipf_requests
+    (persistent) and the one-launch-per-document servers.  Requests are
+    documents drawn from the served model's own topics (model_requests); each
+    server folds in the first half of every document, and the second halves
+    are scored by document completion (completion_loglik) with the theta each
+    server returned, on the requests both servers ran.  Returns the per-rate
+    rows and the held-out log-likelihood per token of both servers, beside
+    that of a uniform theta."""
+    from gpupolyaurnlda_b200.serve import completion_loglik, model_requests, split_halves
+    K = srv_b.K
     rows = []
-    ll_b_all, ll_u_all, tok_all = [], [], []
+    acc = {"batched": [0.0, 0], "unbatched": [0.0, 0], "uniform theta": [0.0, 0]}
     for rate in rates:
         n = int(min(max(seconds * rate, 2000), max_requests))
-        lengths, words = zipf_requests(n, srv_b.V, seed=rate)
+        full_len, full_words = model_requests(q, K, n, seed=rate, device=f"cuda:{local}")
+        lengths, words, h_len, h_words = split_halves(full_len, full_words)
         rng = np.random.default_rng(rate + 1)
         arrival = np.cumsum(rng.exponential(1.0 / rate, n))
         ids = np.arange(n, dtype=np.uint64) + np.uint64(rate) * np.uint64(1 << 32)
+        nu = min(n, max_unbatched)
         clocks = ClockSampler(local)
         clocks.start()
-        dps_b, lat_b, ll_b, sk_b = serve_open_loop(srv_b, lengths, words, arrival, ids)
+        dps_b, lat_b, ll_b, sk_b, th_b = serve_open_loop(srv_b, lengths, words, arrival, ids, keep_theta=nu)
         clk = clocks.stop()
-        nu = min(n, max_unbatched)
-        dps_u, lat_u, ll_u, sk_u = serve_open_loop(srv_u, lengths[:nu], words[:int(lengths[:nu].sum())],
-                                                   arrival[:nu], ids[:nu])
-        same = bool((ll_b[:nu] == ll_u).all() and (sk_b[:nu] == sk_u).all())
-        ll_b_all.append(ll_b[:nu].sum())
-        ll_u_all.append(ll_u.sum())
-        tok_all.append(float((lengths[:nu].astype(np.int64) - sk_u).sum()))
-        rows.append({"offered_docs_per_sec": rate, "requests": n, "tokens": int(lengths.sum()),
+        dps_u, lat_u, ll_u, sk_u, th_u = serve_open_loop(srv_u, lengths[:nu], words[:int(lengths[:nu].sum())],
+                                                         arrival[:nu], ids[:nu], keep_theta=nu)
+        same = bool((ll_b[:nu] == ll_u).all() and (sk_b[:nu] == sk_u).all() and
+                    (th_b.view(np.uint32) == th_u.view(np.uint32)).all())
+        hw = h_words[:int(h_len[:nu].astype(np.int64).sum())]
+        for name, th in (("batched", th_b), ("unbatched", th_u), ("uniform theta", np.full_like(th_b, 1.0 / K))):
+            tot, cnt = completion_loglik(q, K, th, h_len[:nu], hw, device=f"cuda:{local}")
+            acc[name][0] += tot
+            acc[name][1] += cnt
+        rows.append({"offered_docs_per_sec": rate, "requests": n, "tokens_folded_in": int(lengths.sum()),
                      "batched": {"docs_per_sec": dps_b, "p50_ms": float(np.percentile(lat_b, 50) / 1e6),
                                  "p99_ms": float(np.percentile(lat_b, 99) / 1e6)},
                      "unbatched": {"requests": nu, "docs_per_sec": dps_u,
                                    "p50_ms": float(np.percentile(lat_u, 50) / 1e6),
                                    "p99_ms": float(np.percentile(lat_u, 99) / 1e6)},
                      "results_identical": same, "clocks": clk})
-    llb, llu = sum(ll_b_all) / sum(tok_all), sum(ll_u_all) / sum(tok_all)
-    return rows, {"batched": llb, "unbatched": llu, "rel_diff": abs(llb - llu) / abs(llu)}
+    ll = {k: v[0] / max(1, v[1]) for k, v in acc.items()}
+    ll["rel_diff"] = abs(ll["batched"] - ll["unbatched"]) / abs(ll["unbatched"])
+    ll["tokens_scored"] = acc["batched"][1]
+    ll["definition"] = ("document completion: fold in the first ceil(L/2) tokens (50 iterations, Phi fixed), "
+                        "score the rest by log sum_k theta_k Phi[k][w] per token")
+    return rows, ll
 
 
-SERVE_WORKLOAD = ("50 fold-in iterations per request, Zipf(1.05) documents, lengths lognormal(5.0,1.2) clipped "
-                  "[5,20000], Poisson arrivals")
+SERVE_WORKLOAD = ("documents drawn from the served model's topics (theta ~ Dir(0.1)), lengths lognormal(5.0,1.2) "
+                  "clipped [5,20000], the first half of each folded in with 50 iterations, Poisson arrivals")
 
 
 def run_serve(args):
@@ -634,9 +753,10 @@ def run_serve(args):
     s.corpus_sweep(args.serve_train)
     srv_b = Server(50, seed=0, max_inflight=1 << 17)  # persistent: 32 request warps per SM
     srv_u = Server(50, mode="launch", slots=args.serve_slots, max_batch=1, seed=0)
+    q_model = s.read_state(n=False, alias=False, A=False, S=False, nnz=False)["q"]
     s.close()
     del c
-    rows, ll = serve_measure(srv_b, srv_u, args.rates, args.serve_seconds, args.serve_requests,
+    rows, ll = serve_measure(srv_b, srv_u, q_model, args.rates, args.serve_seconds, args.serve_requests,
                              args.serve_unbatched, local)
     st_b = srv_b.stats()
     srv_b.close()
@@ -698,7 +818,7 @@ def run_sharded(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u64",
                 "data": "synthetic",
-                "config": dict(workload_desc(c, args), parallelism=f"document shards x{world} + count all-reduce"),
+                "config": workload_desc(c, args), "parallelism": f"document shards x{world} + count all-reduce",
                 "timing": "wall clock around the timed iterations (each ends with a host synchronisation), max over "
                           "ranks", "clocks": clk}
         print(json.dumps(line), flush=True)

@@ -155,6 +155,7 @@ _SIGNATURES = {
     "gpulda_batch_get_shapes": (C.c_int, [C.c_void_p, C.POINTER(BatchShape)]),
     "gpulda_batch_set_shapes": (C.c_int, [C.c_void_p, C.POINTER(BatchShape)]),
     "gpulda_batch_tune": (C.c_int, [C.c_void_p, C.c_char_p, _U32P]),
+    "gpulda_batch_set_mode": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "gpulda_batch_info": (C.c_int, [C.c_void_p, _U64P, C.c_int]),
     # include/gpulda_serve.h
     "gpulda_serve_create": (C.c_int, [C.POINTER(ServeArgs), C.POINTER(C.c_void_p)]),

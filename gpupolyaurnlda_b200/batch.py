@@ -111,6 +111,14 @@ class BatchChains:
             arr[i] = BatchShape(a, b, c, 0)
         check(lib().gpulda_batch_set_shapes(self.h, arr), "batch set_shapes")
 
+    def set_mode(self, merged: bool, shape: tuple[int, int, int] | None = None) -> None:
+        """Merged mode (one launch per stage over every problem) or per-bucket
+        mode; `shape` sets the merged launches' (z warps per block, z blocks
+        per SM, Poisson cells per block)."""
+        sh = BatchShape(shape[0], shape[1], shape[2], 0) if shape else None
+        check(lib().gpulda_batch_set_mode(self.h, 1 if merged else 0, C.byref(sh) if sh else None),
+              "batch set_mode")
+
     def tune(self, cache_path: str | None = None) -> int:
         n = C.c_uint32(0)
         check(lib().gpulda_batch_tune(self.h, cache_path.encode() if cache_path else None, C.byref(n)),
@@ -118,9 +126,9 @@ class BatchChains:
         return int(n.value)
 
     def info(self) -> dict:
-        out = (C.c_uint64 * 8)()
-        m = lib().gpulda_batch_info(self.h, out, 8)
-        keys = ("problems", "tokens", "docs", "words", "cells", "device_bytes", "buckets", "iterations")
+        out = (C.c_uint64 * 9)()
+        m = lib().gpulda_batch_info(self.h, out, 9)
+        keys = ("problems", "tokens", "docs", "words", "cells", "device_bytes", "buckets", "iterations", "merged")
         return {k: int(out[i]) for i, k in enumerate(keys[:m])}
 
 

@@ -10,10 +10,16 @@
 // so that a bucket's cells, words, documents and tokens are contiguous.  The
 // iteration graph is
 //   bump t; zero S, log-likelihood sums, counters and work counters;
-//   per bucket, as concurrent branches:
-//     phi_draw_batch -> alias_build_batch -> z_sweep_kernel<BATCH>
+//   merged mode (the default): one launch per stage over every problem --
+//     phi_draw_batch over all problems' rows, alias_build_batch over all
+//     words, and one z_sweep_kernel<BATCH> whose persistent warps take
+//     (problem, document) items longest first from one work queue spanning
+//     all buckets, shared memory sized for the largest K;
+//   per-bucket mode: per bucket, as concurrent branches,
+//     phi_draw_batch -> alias_build_batch -> z_sweep_kernel<BATCH>;
 // and every kernel reads t from device memory, so the graph is captured once
-// and replayed for every iteration.
+// and replayed for every iteration.  The autotuner picks launch shapes per
+// bucket and for the merged launches, and the faster mode.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -97,11 +103,21 @@ struct Slot {  // one problem, in arena order
   u32 word0, doc0;
 };
 
+// Index of the merged launches' work counter (after the buckets').
+constexpr u32 kMergedWork = GPULDA_BATCH_BUCKETS;
+
 struct Batch {
   u32 P = 0;
   std::vector<Slot> slots;
   std::vector<u32> slot_of;  // user index -> slot
   Bucket bk[GPULDA_BATCH_BUCKETS];
+  // merged mode: one launch per stage over every problem
+  bool merged = true;
+  GpuldaBatchShape mshape{8, 0, 65536, 0};
+  u32 Kmax_all = 0;
+  bool want_ll_all = false;
+  u32 mblock0 = 0, m_n_blocks = 0;  // Poisson-draw block table section of the merged launch
+  u32* order_all = nullptr;          // every document, longest first
   u64 cells = 0, N = 0, S_total = 0;
   u32 D = 0, Vtot = 0;
   u64 bytes = 0;
@@ -184,14 +200,24 @@ std::vector<uint4> block_table(const Batch& b, const Bucket& bu, u32 cells) {
   return out;
 }
 
-// Rebuilds every bucket's block table for its current shape.
+// Rebuilds every bucket's block table for its current shape, then the merged
+// launch's table (every problem) for the merged shape.
 int upload_block_tables(Batch& b) {
   std::vector<uint4> all;
+  Bucket every;
+  every.slot0 = 0;
+  every.slot1 = b.P;
   for (auto& bu : b.bk) {
     if (!bu.used) continue;
     std::vector<uint4> t = block_table(b, bu, bu.shape.phi_cells_per_block);
     bu.block0 = (u32)all.size();
     bu.n_blocks = (u32)t.size();
+    all.insert(all.end(), t.begin(), t.end());
+  }
+  {
+    std::vector<uint4> t = block_table(b, every, b.mshape.phi_cells_per_block);
+    b.mblock0 = (u32)all.size();
+    b.m_n_blocks = (u32)t.size();
     all.insert(all.end(), t.begin(), t.end());
   }
   if (all.size() > b.blocks_cap) {
@@ -228,6 +254,25 @@ ZLaunch z_args(const Batch& b, u32 j, unsigned long long* counters, double* ll) 
   return zl;
 }
 
+// The merged launches' z-sweep arguments: every document, longest first.
+ZLaunch z_args_merged(const Batch& b, unsigned long long* counters, double* ll) {
+  ZLaunch zl = z_args(b, 0, counters, ll);
+  zl.order = b.order_all;
+  zl.n_docs = b.D;
+  zl.flags = b.want_ll_all ? 1u : 0u;
+  zl.work = b.work + kMergedWork;
+  return zl;
+}
+
+// One launch per stage over every problem on stream s (work counter zeroed by
+// the caller).
+void merged_iteration(const Batch& b, cudaStream_t s) {
+  launch_phi_draw_batch(b.ar, b.phidev(b.mblock0), b.m_n_blocks, b.Kmax_all, b.t_dev, s);
+  launch_alias_build_batch(b.ar, b.phidev(b.mblock0), b.Kmax_all, 0, b.Vtot, s);
+  launch_z_sweep_batch(b.ar, b.zdev(), b.Kmax_all, z_args_merged(b, b.counters, b.ll), s, b.mshape.z_warps_per_block,
+                       b.mshape.z_blocks_per_sm);
+}
+
 // The bucket's three kernels on stream s (work counter zeroed by the caller).
 void bucket_iteration(const Batch& b, u32 j, cudaStream_t s) {
   const Bucket& bu = b.bk[j];
@@ -245,15 +290,19 @@ int capture_graph(Batch& b) {
   cudaMemsetAsync(b.ar.S, 0, b.S_total * 8, s);
   cudaMemsetAsync(b.ll, 0, (size_t)b.P * 16, s);
   cudaMemsetAsync(b.counters, 0, kCtrN * 8, s);
-  cudaMemsetAsync(b.work, 0, GPULDA_BATCH_BUCKETS * 4, s);
-  cudaEventRecord(b.fork, s);
-  for (u32 j = 0; j < GPULDA_BATCH_BUCKETS; ++j) {
-    Bucket& bu = b.bk[j];
-    if (!bu.used) continue;
-    cudaStreamWaitEvent(bu.s, b.fork, 0);
-    bucket_iteration(b, j, bu.s);
-    cudaEventRecord(bu.join, bu.s);
-    cudaStreamWaitEvent(s, bu.join, 0);
+  cudaMemsetAsync(b.work, 0, (GPULDA_BATCH_BUCKETS + 1) * 4, s);
+  if (b.merged) {
+    merged_iteration(b, s);
+  } else {
+    cudaEventRecord(b.fork, s);
+    for (u32 j = 0; j < GPULDA_BATCH_BUCKETS; ++j) {
+      Bucket& bu = b.bk[j];
+      if (!bu.used) continue;
+      cudaStreamWaitEvent(bu.s, b.fork, 0);
+      bucket_iteration(b, j, bu.s);
+      cudaEventRecord(bu.join, bu.s);
+      cudaStreamWaitEvent(s, bu.join, 0);
+    }
   }
   const cudaError_t launch_err = cudaGetLastError();
   cudaGraph_t g = nullptr;
@@ -366,6 +415,8 @@ int create_impl(const GpuldaProblem* probs, u32 P, Batch** out) {
     bu.tok1 = N;
     bu.Kmax = std::max(bu.Kmax, p.K);
     bu.want_ll = bu.want_ll || (p.flags & GPULDA_FLAG_LOGLIK);
+    b.Kmax_all = std::max(b.Kmax_all, p.K);
+    b.want_ll_all = b.want_ll_all || (p.flags & GPULDA_FLAG_LOGLIK);
   }
   b.cells = cells;
   b.S_total = S;
@@ -387,6 +438,7 @@ int create_impl(const GpuldaProblem* probs, u32 P, Batch** out) {
       (rc = b.alloc(&ar.csr, cells)) || (rc = b.alloc(&ar.A, W)) || (rc = b.alloc(&ar.S, S)) ||
       (rc = b.alloc(&ar.nnz, W)) || (rc = b.alloc(&b.z, N)) || (rc = b.alloc(&b.w, N)) ||
       (rc = b.alloc(&b.d_len, D)) || (rc = b.alloc(&b.d_idx, D)) || (rc = b.alloc(&b.order, D)) ||
+      (rc = b.alloc(&b.order_all, D)) ||
       (rc = b.alloc(&b.pid, D)) || (rc = b.alloc(&b.wpid, W)) || (rc = b.alloc(&b.row_off, W)) ||
       (rc = b.alloc(&b.K, P)) || (rc = b.alloc(&b.key0, P)) || (rc = b.alloc(&b.key1, P)) ||
       (rc = b.alloc(&b.alpha, P)) || (rc = b.alloc(&b.beta, P)) || (rc = b.alloc(&b.tok_base, P)) ||
@@ -394,7 +446,7 @@ int create_impl(const GpuldaProblem* probs, u32 P, Batch** out) {
       (rc = b.alloc(&b.lg_Ka, P)) || (rc = b.alloc(&b.cdf, (size_t)P * kPoisN * kPoisW)) ||
       (rc = b.alloc(&b.guide, (size_t)P * kPoisN * 256)) || (rc = b.alloc(&b.lfac, (size_t)P * kLogFacN)) ||
       (rc = b.alloc(&b.t_dev, 1)) || (rc = b.alloc(&b.ll, 2 * (size_t)P)) || (rc = b.alloc(&b.counters, kCtrN)) ||
-      (rc = b.alloc(&b.work, GPULDA_BATCH_BUCKETS)) || (rc = b.alloc(&b.status, 1)))
+      (rc = b.alloc(&b.work, GPULDA_BATCH_BUCKETS + 1)) || (rc = b.alloc(&b.status, 1)))
     return rc;
 
   // Every upload is ordered on the batch stream: a pageable cudaMemcpy may
@@ -483,6 +535,19 @@ int create_impl(const GpuldaProblem* probs, u32 P, Batch** out) {
     for (size_t i = 0; i < len.size(); ++i) order[bu.doc0 + i] = len[i].second;
   }
   if (D) BCK(cudaMemcpyAsync(b.order, order.data(), (size_t)D * 4, cudaMemcpyHostToDevice, b.stream));
+  // every document, longest first (stable), for the merged launch
+  std::vector<u32> order_all(D);
+  {
+    std::vector<u32> lens(D);
+    for (u32 si = 0; si < P; ++si) {
+      const Slot& sl = b.slots[si];
+      const GpuldaProblem& p = probs[sl.user];
+      for (u32 d = 0; d < sl.n_docs; ++d) lens[sl.doc0 + d] = p.d_len[d];
+    }
+    for (u32 d = 0; d < D; ++d) order_all[d] = d;
+    std::stable_sort(order_all.begin(), order_all.end(), [&](u32 x, u32 y) { return lens[x] > lens[y]; });
+  }
+  if (D) BCK(cudaMemcpyAsync(b.order_all, order_all.data(), (size_t)D * 4, cudaMemcpyHostToDevice, b.stream));
   static const u32 t0 = 0xffffffffu;  // the first bump makes it iteration 0
   BCK(cudaMemcpyAsync(b.t_dev, &t0, 4, cudaMemcpyHostToDevice, b.stream));
   BCK(cudaMemsetAsync(b.status, 0, 4, b.stream));
@@ -670,6 +735,105 @@ int tune_bucket(Batch& b, u32 j) {
   return rc2;
 }
 
+// Tunes the merged launches' shape on the batch's own data, then times one
+// whole iteration in each mode and keeps the faster.  All counts and topics
+// are saved first and restored at the end, and the iteration counter is put
+// back, so the chains are unaffected.
+int tune_merged(Batch& b) {
+  cudaStream_t s = b.stream;
+  u32 *n_save = nullptr, *z_save = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = GPULDA_OK;
+  BCK(cudaMalloc(&n_save, std::max<u64>(1, b.cells) * 4));
+  if (cudaMalloc(&z_save, std::max<u64>(1, b.N) * 4) != cudaSuccess) {
+    cudaFree(n_save);
+    return report_error(GPULDA_ERR_NOMEM, "autotuner snapshot");
+  }
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const u32 t_next = (u32)(b.t + 1), t_cur = (u32)b.t;
+  const GpuldaBatchShape keep = b.mshape;
+  const bool keep_mode = b.merged;
+  GpuldaBatchShape best = keep;
+  bool best_merged = keep_mode;
+  float best_phi = 1e30f, best_z = 1e30f;
+  auto restore = [&]() -> int {
+    BCK(cudaMemcpyAsync(b.ar.n, n_save, b.cells * 4, cudaMemcpyDeviceToDevice, s));
+    BCK(cudaMemcpyAsync(b.z, z_save, b.N * 4, cudaMemcpyDeviceToDevice, s));
+    return GPULDA_OK;
+  };
+  auto run = [&]() -> int {
+    BCK(cudaMemcpyAsync(n_save, b.ar.n, b.cells * 4, cudaMemcpyDeviceToDevice, s));
+    BCK(cudaMemcpyAsync(z_save, b.z, b.N * 4, cudaMemcpyDeviceToDevice, s));
+    BCK(cudaMemcpyAsync(b.t_dev, &t_next, 4, cudaMemcpyHostToDevice, s));
+    BCK(cudaStreamSynchronize(s));
+    const u32 phi_c[] = {16384, 65536, 262144};
+    for (u32 c : phi_c) {
+      b.mshape.phi_cells_per_block = c;
+      if ((rc = upload_block_tables(b))) return rc;
+      if ((rc = restore())) return rc;
+      BCK(cudaMemsetAsync(b.ar.S, 0, b.S_total * 8, s));
+      float ms = 0;
+      if ((rc = time_on(s, e0, e1, [&] {
+             launch_phi_draw_batch(b.ar, b.phidev(b.mblock0), b.m_n_blocks, b.Kmax_all, b.t_dev, s);
+           }, &ms)))
+        return rc;
+      if (ms < best_phi) {
+        best_phi = ms;
+        best.phi_cells_per_block = c;
+      }
+    }
+    launch_alias_build_batch(b.ar, b.phidev(b.mblock0), b.Kmax_all, 0, b.Vtot, s);
+    BCK(cudaGetLastError());
+    const u32 zc[][2] = {{8, 0}, {4, 0}, {2, 0}, {8, 2}, {4, 4}};
+    for (const auto& c : zc) {
+      BCK(cudaMemcpyAsync(b.z, z_save, b.N * 4, cudaMemcpyDeviceToDevice, s));
+      BCK(cudaMemsetAsync(b.ar.n, 0, b.cells * 4, s));
+      BCK(cudaMemsetAsync(b.work + kMergedWork, 0, 4, s));
+      ZLaunch zl = z_args_merged(b, b.counters, nullptr);
+      zl.flags = 0;
+      float ms = 0;
+      if ((rc = time_on(s, e0, e1, [&] { launch_z_sweep_batch(b.ar, b.zdev(), b.Kmax_all, zl, s, c[0], c[1]); },
+                        &ms)))
+        return rc;
+      if (ms < best_z) {
+        best_z = ms;
+        best.z_warps_per_block = c[0];
+        best.z_blocks_per_sm = c[1];
+      }
+    }
+    // one whole iteration in each mode, from the same state
+    b.mshape = best;
+    if ((rc = upload_block_tables(b))) return rc;
+    float mode_ms[2] = {1e30f, 1e30f};
+    for (int m = 0; m < 2; ++m) {
+      b.merged = m == 1;
+      b.drop_graph();
+      if ((rc = capture_graph(b))) return rc;
+      if ((rc = restore())) return rc;
+      BCK(cudaMemcpyAsync(b.t_dev, &t_cur, 4, cudaMemcpyHostToDevice, s));  // the graph bumps it to t + 1
+      if ((rc = time_on(s, e0, e1, [&] { cudaGraphLaunch(b.exec, s); }, &mode_ms[m]))) return rc;
+    }
+    best_merged = mode_ms[1] <= mode_ms[0];
+    return GPULDA_OK;
+  };
+  rc = run();
+  restore();
+  cudaMemcpyAsync(b.t_dev, &t_cur, 4, cudaMemcpyHostToDevice, s);
+  const cudaError_t e = cudaStreamSynchronize(s);
+  cudaFree(n_save);
+  cudaFree(z_save);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b.mshape = rc ? keep : best;
+  b.merged = rc ? keep_mode : best_merged;
+  b.drop_graph();
+  const int rc2 = upload_block_tables(b);
+  if (rc) return rc;
+  if (e != cudaSuccess) return report_cuda_error(e, "autotuner restore");
+  return rc2;
+}
+
 Batch* as_batch(void* h) { return static_cast<Batch*>(h); }
 
 }  // namespace
@@ -769,6 +933,22 @@ extern "C" int gpulda_batch_set_shapes(void* handle, const GpuldaBatchShape* sha
   return upload_block_tables(*b);
 }
 
+extern "C" int gpulda_batch_set_mode(void* handle, uint32_t mode, const GpuldaBatchShape* merged_shape) {
+  Batch* b = as_batch(handle);
+  if (!b || mode > GPULDA_BATCH_MERGED) return report_error(GPULDA_ERR_ARGS, "bad batch set_mode arguments");
+  if (merged_shape) {
+    const GpuldaBatchShape& sh = *merged_shape;
+    if ((sh.z_warps_per_block != 2 && sh.z_warps_per_block != 4 && sh.z_warps_per_block != 8) ||
+        sh.phi_cells_per_block < 1)
+      return report_error(GPULDA_ERR_ARGS, "shape: z_warps_per_block must be 2, 4 or 8, phi cells positive");
+  }
+  BCK(cudaDeviceSynchronize());
+  b->merged = mode == GPULDA_BATCH_MERGED;
+  if (merged_shape) b->mshape = *merged_shape;
+  b->drop_graph();
+  return upload_block_tables(*b);
+}
+
 extern "C" int gpulda_batch_tune(void* handle, const char* cache_path, uint32_t* n_tuned) {
   Batch* b = as_batch(handle);
   if (!b) return report_error(GPULDA_ERR_ARGS, "null batch handle");
@@ -793,6 +973,25 @@ extern "C" int gpulda_batch_tune(void* handle, const char* cache_path, uint32_t*
     ++tuned;
     changed = true;
   }
+  // the merged launches' shape and the mode, for this batch's composition
+  // (bucket bounds present and total size in millions of tokens)
+  std::string comp;
+  for (u32 j = 0; j < GPULDA_BATCH_BUCKETS; ++j)
+    if (b->bk[j].used) comp += std::to_string(kBucketBound[j]) + ",";
+  const std::string mkey = dev + "|merged|" + comp + "N~" + std::to_string(b->N >> 20);
+  auto it = cache.find(mkey);
+  if (it != cache.end() && it->second.size() >= 4 &&
+      (it->second[0] == 2 || it->second[0] == 4 || it->second[0] == 8) && it->second[2] > 0) {
+    b->mshape = GpuldaBatchShape{(u32)it->second[0], (u32)it->second[1], (u32)it->second[2], 0};
+    b->merged = it->second[3] != 0;
+  } else {
+    const int rc = tune_merged(*b);
+    if (rc) return rc;
+    cache[mkey] = {b->mshape.z_warps_per_block, b->mshape.z_blocks_per_sm, b->mshape.phi_cells_per_block,
+                   b->merged ? 1ul : 0ul};
+    ++tuned;
+    changed = true;
+  }
   b->drop_graph();
   int rc = upload_block_tables(*b);
   if (rc) return rc;
@@ -807,8 +1006,8 @@ extern "C" int gpulda_batch_info(void* handle, uint64_t* out, int n) {
   if (!b || !out) return 0;
   u32 used = 0;
   for (auto& bu : b->bk) used += bu.used;
-  const uint64_t v[8] = {b->P, b->N, b->D, b->Vtot, b->cells, b->bytes, used, b->iters};
-  const int m = n < 8 ? n : 8;
+  const uint64_t v[9] = {b->P, b->N, b->D, b->Vtot, b->cells, b->bytes, used, b->iters, b->merged ? 1u : 0u};
+  const int m = n < 9 ? n : 9;
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;
 }

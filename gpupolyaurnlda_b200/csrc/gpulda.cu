@@ -154,6 +154,11 @@ struct Model {
   bool phi_timed = false, z_timed = false;
   cudaEvent_t z_ev[3] = {};
   u32 launches = 0;
+  // Recorded on the caller's stream after each allocation-free sweep; the
+  // library's own stream work that reads or resets what that sweep writes
+  // (counts, statistics, log-likelihood) waits for it.
+  cudaEvent_t noalloc_done = nullptr;
+  bool noalloc_pending = false;
 
   // device-resident corpus
   u32 *cz = nullptr, *cw = nullptr, *cd_len = nullptr, *cd_idx = nullptr, *cK_d = nullptr, *corder = nullptr;
@@ -254,6 +259,7 @@ void free_model() {
   if (g.side) cudaStreamDestroy(g.side);
   if (g.fork) cudaEventDestroy(g.fork);
   if (g.join) cudaEventDestroy(g.join);
+  if (g.noalloc_done) cudaEventDestroy(g.noalloc_done);
   const int fatal = g.fatal;
   g = Model();
   g.fatal = fatal;
@@ -292,6 +298,7 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
   CK(cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&g.fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&g.noalloc_done, cudaEventDisableTiming));
   for (auto& e : g.ev) CK(cudaEventCreate(&e));
   for (auto& e : g.z_ev) CK(cudaEventCreate(&e));
   if ((rc = dalloc(&g.dev.n, cells)) || (rc = dalloc(&g.dev.q, cells)) || (rc = dalloc(&g.dev.al, cells)) ||
@@ -371,8 +378,16 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
   return GPULDA_OK;
 }
 
+// Orders work about to be issued on `s` after the last allocation-free sweep,
+// which ran on a stream of the caller's choosing.
+int after_noalloc(cudaStream_t s) {
+  if (g.noalloc_pending) CK(cudaStreamWaitEvent(s, g.noalloc_done, 0));
+  return GPULDA_OK;
+}
+
 // Phi step on `s` without a host synchronisation.
 int phi_step_async(cudaStream_t s) {
+  if (int rc = after_noalloc(s)) return rc;
   g.t += 1;
   g.tok_offset = g.shard_base;
   g.swept = false;
@@ -974,7 +989,10 @@ extern "C" int gpulda_debug_alias(const uint32_t* q, uint32_t K, uint64_t* table
 // device with cudaGetSymbolAddress (on the first call on that device, which
 // is why that first call should come before any stream capture).  All calls
 // share the array, so calls whose work overlaps on the GPU race with each
-// other; the work-queue counter is cleared on every call.
+// other; the work-queue counter is cleared on every call.  Calls issued one
+// after another from the host are ordered on the GPU even on different
+// streams (each waits for the previous call's event), and the next Phi step
+// waits for the last call, so the counts it reads are complete.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr u32 kNoAllocMaxDocs = GPULDA_NOALLOC_MAX_DOCS;
@@ -1007,6 +1025,8 @@ extern "C" int gpulda_sample_z_device_noalloc(uint32_t* z, const uint32_t* w, co
   u32* d_idx = g_noalloc_addr[dev];
   u32* work = d_idx + kNoAllocMaxDocs;
   cudaStream_t s = stream ? (cudaStream_t)stream : main_stream();
+  // the previous call's use of the shared scratch ends before this one's begins
+  if (int rc = after_noalloc(s)) return rc;
   CK(cudaMemsetAsync(work, 0, sizeof(u32), s));
   launch_doc_offsets(d_len, d_idx, n_docs, s);
   CK(cudaGetLastError());
@@ -1026,8 +1046,18 @@ extern "C" int gpulda_sample_z_device_noalloc(uint32_t* z, const uint32_t* w, co
   zl.ll = g.ll;
   zl.work = work;
   zl.status = g.status;
-  launch_z_sweep(g.dev, zl, s);
+  // Above kMapMinK topics, the large-K store the other sweeps use.  The
+  // lengths are on the device only, so the launch accepts any document length
+  // and sizes each document's store for K distinct topics.
+  bool done = false;
+  if (g.K > kMapMinK)
+    done = (g.flags & GPULDA_FLAG_HASHMAP) ? launch_z_sweep_map(g.dev, zl, s, 65535u)
+                                           : launch_z_sweep_pairs(g.dev, zl, s, 65535u);
+  if (!done) launch_z_sweep(g.dev, zl, s);
   CK(cudaGetLastError());
+  CK(cudaEventRecord(g.noalloc_done, s));
+  g.noalloc_pending = true;
+  g.launches += 2;
   g.tok_offset += n_tokens;
   g.swept = true;
   return GPULDA_OK;

@@ -335,7 +335,10 @@ __global__ void __launch_bounds__(1024) doc_offsets_kernel(const u32* __restrict
   u64 total;
   u64 off = block_excl_scan_u64(s, sh, &total);
   for (u32 i = i0; i < i1; ++i) {
-    d_idx[i] = (u32)off;
+    // Saturate instead of wrapping: buffers hold fewer than 2^32 tokens, so an
+    // offset of 2^32 - 1 fails the sweep's range check (offset + length must
+    // not pass n_tokens) and is reported, where a wrapped offset could pass it.
+    d_idx[i] = off < 0xffffffffull ? (u32)off : 0xffffffffu;
     off += d_len[i];
   }
 }

@@ -116,4 +116,79 @@ def zipf_requests(n: int, V: int, seed: int, mu: float = 5.0, sigma: float = 1.2
     return lengths, words
 
 
-__all__ = ["Server", "zipf_requests"]
+def model_requests(q: np.ndarray, K: int, n: int, seed: int, doc_conc: float = 0.1, mu: float = 5.0,
+                   sigma: float = 1.2, lo: int = 5, hi: int = 20000, device: str = "cuda"):
+    """Synthetic requests drawn from a model's own topics (the LDA generative
+    process): per document theta ~ Dirichlet(doc_conc), lengths
+    round(lognormal(mu, sigma)) clipped to [lo, hi], each token's topic from
+    theta and its word from that topic's Phi column, Phi[k][w] =
+    q[w][k] / sum_w q[w][k] (q: the V x K word-major fixed-point Phi).
+    Returns (lengths u32, words u32)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    V = len(q) // K
+    lengths = np.clip(np.round(rng.lognormal(mu, sigma, n)), lo, hi).astype(np.uint32)
+    theta = rng.dirichlet(np.full(K, doc_conc), n)
+    z = np.concatenate([rng.choice(K, int(L), p=th / th.sum()) for L, th in zip(lengths, theta)]).astype(np.int64)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    qt = torch.from_numpy(np.ascontiguousarray(q, np.uint32).view(np.int32)).to(device).view(V, K)
+    words = np.empty(len(z), np.uint32)
+    zt = torch.from_numpy(z).to(device)
+    order = torch.argsort(zt)
+    zs = zt[order]
+    bounds = torch.searchsorted(zs, torch.arange(K + 1, device=device)).cpu().numpy()
+    out = torch.empty(len(z), dtype=torch.int64, device=device)
+    for k0 in range(0, K, 64):  # topic columns in blocks: a K x V float64 table is not needed at once
+        k1 = min(K, k0 + 64)
+        col = (qt[:, k0:k1].to(torch.int64) & 0xffffffff).to(torch.float64).t()  # (k1-k0) x V
+        cdf = torch.cumsum(col, dim=1)
+        tot = cdf[:, -1:].clamp_min(1.0)
+        cdf = cdf / tot + torch.arange(k1 - k0, device=device, dtype=torch.float64)[:, None]
+        flat = cdf.reshape(-1)
+        a, b = int(bounds[k0]), int(bounds[k1])
+        if b > a:
+            kk = zs[a:b] - k0
+            u = torch.rand(b - a, dtype=torch.float64, device=device, generator=g)
+            idx = torch.searchsorted(flat, kk.double() + u, right=True).clamp_max(flat.numel() - 1)
+            out[order[a:b]] = (idx - kk * V).clamp_(0, V - 1)
+    words[:] = out.cpu().numpy().astype(np.uint32)
+    return lengths, words
+
+
+def split_halves(lengths: np.ndarray, words: np.ndarray):
+    """Document completion: the first ceil(L/2) tokens of every document are
+    folded in, the rest are scored.  Returns (first lengths, first words,
+    second lengths, second words)."""
+    lengths = np.asarray(lengths, np.int64)
+    first = (lengths + 1) // 2
+    offs = np.concatenate([[0], np.cumsum(lengths)])
+    in_first = np.arange(offs[-1]) - np.repeat(offs[:-1], lengths) < np.repeat(first, lengths)
+    return (first.astype(np.uint32), np.ascontiguousarray(words[in_first], np.uint32),
+            (lengths - first).astype(np.uint32), np.ascontiguousarray(words[~in_first], np.uint32))
+
+
+def completion_loglik(q: np.ndarray, K: int, theta: np.ndarray, lengths: np.ndarray, words: np.ndarray,
+                      device: str = "cuda") -> tuple[float, int]:
+    """Held-out log-likelihood of document completion: sum over every scored
+    token i of document d of log sum_k theta[d][k] Phi[k][w_i], with Phi[k][w]
+    = q[w][k] / 2^32 (the fixed-point Phi the fold-in used).  theta is
+    n x K (float), lengths/words the scored tokens.  Returns (sum, tokens
+    scored); tokens whose mixture is zero are not scored."""
+    import torch
+    V = len(q) // K
+    qt = torch.from_numpy(np.ascontiguousarray(q, np.uint32).view(np.int32)).to(device).view(V, K)
+    th = torch.from_numpy(np.ascontiguousarray(theta, np.float32)).to(device).double()
+    doc = torch.from_numpy(np.repeat(np.arange(len(lengths)), np.asarray(lengths, np.int64))).to(device)
+    wt = torch.from_numpy(np.asarray(words, np.int64)).to(device)
+    total, scored = 0.0, 0
+    for a in range(0, len(wt), 1 << 16):
+        rows = (qt[wt[a:a + (1 << 16)]].to(torch.int64) & 0xffffffff).double() / 4294967296.0
+        p = (rows * th[doc[a:a + (1 << 16)]]).sum(dim=1)
+        ok = p > 0
+        total += float(torch.log(p[ok]).sum())
+        scored += int(ok.sum())
+    return total, scored
+
+
+__all__ = ["Server", "zipf_requests", "model_requests", "split_halves", "completion_loglik"]

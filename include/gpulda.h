@@ -243,11 +243,19 @@ int gpulda_debug_alias(const uint32_t* q, uint32_t K, uint64_t* table_out);
  * it is serving, or work issued where cudaMalloc is not permitted).
  *
  * Sweeps n_docs documents whose topics z (read and rewritten), words w and
- * lengths d_len are already in device memory, exactly as sample_z_async
- * sweeps a buffer (same draws, same count rebuild, continuing the current
- * iteration's token numbering).  Asynchronous on `stream` (NULL: the
- * library's stream); device-side input errors are reported by the next
- * sync_buffer / sample_phi / gpulda_corpus_* call.
+ * lengths d_len are already in device memory with the draws and count rebuild
+ * of sample_z_async, continuing the current iteration's token numbering (for
+ * K above 2048 with the large-K store sized for K distinct topics per
+ * document).  Asynchronous on `stream` (NULL: the library's stream); device-side
+ * input errors are reported by the next sync_buffer / sample_phi /
+ * gpulda_corpus_* call.  Per-document distinct-topic counts (K_d) are not
+ * written and gpulda_kernel_times does not cover this call.
+ *
+ * Ordering: the next sample_phi (and gpulda_corpus_sweep) waits on the GPU
+ * for the last allocation-free sweep, whatever stream it ran on, so the caller
+ * need not synchronize its stream before sample_phi; gpulda_loglik,
+ * gpulda_counters and gpulda_debug_read synchronize the device.  Calls made
+ * one after another from the host are ordered on the GPU as well.
  *
  * It allocates nothing: its scratch (document offsets and a work counter) is
  * a fixed device array of the library, 4 MiB + 256 B held by every GPU that
@@ -255,7 +263,8 @@ int gpulda_debug_alias(const uint32_t* q, uint32_t K, uint64_t* table_out);
  * GPULDA_NOALLOC_MAX_DOCS is rejected with GPULDA_ERR_UNSUPPORTED.  The first
  * call on a device looks up that array's address, so make the first call
  * before any stream capture.  Calls share the array: calls whose work
- * overlaps on the GPU race with each other. */
+ * overlaps on the GPU (issued from several host threads, say) race with each
+ * other. */
 #define GPULDA_NOALLOC_MAX_DOCS 1048576u
 int gpulda_sample_z_device_noalloc(uint32_t* z, const uint32_t* w, const uint32_t* d_len, uint32_t n_docs,
                                    uint64_t n_tokens, void* stream);

@@ -13,9 +13,14 @@
  * Layout: all problems' (word, topic) rows, word vectors, per-topic sums,
  * tokens and documents live in shared device arenas, grouped by K bucket
  * (K <= 64, <= 256, <= 1024, <= 2048).  One iteration of every problem is
- * one CUDA graph: per bucket, Poisson draw -> alias build -> z sweep, the
- * buckets as concurrent branches, the iteration number read from device
- * memory so the same graph replays for every iteration.
+ * one CUDA graph, the iteration number read from device memory so the same
+ * graph replays for every iteration.  In the merged mode (the default) the
+ * graph holds one launch per stage for all problems: a Poisson draw over
+ * every problem's rows, an alias build over every word, and one persistent
+ * z sweep whose warps take (problem, document) items, longest first, from a
+ * single work queue spanning all buckets.  In the per-bucket mode each bucket
+ * runs Poisson draw -> alias build -> z sweep as a concurrent branch with its
+ * own launch shapes.  Both modes give the same chains bit for bit.
  *
  * Handles are independent of each other and of the single-model state of
  * gpulda.h.  Calls on one handle come from one host thread.  Errors follow
@@ -52,7 +57,11 @@ typedef struct GpuldaProblem {
 #define GPULDA_BATCH_MAX_K 2048u
 #define GPULDA_BATCH_BUCKETS 4u
 
-/* Launch shapes of one K bucket. */
+/* Modes (gpulda_batch_set_mode). */
+#define GPULDA_BATCH_PER_BUCKET 0u
+#define GPULDA_BATCH_MERGED 1u
+
+/* Launch shapes of one K bucket, or of the merged launches. */
 typedef struct GpuldaBatchShape {
   uint32_t z_warps_per_block;    /* 2, 4 or 8 documents per block */
   uint32_t z_blocks_per_sm;      /* cap on resident blocks per SM, 0: as many as fit */
@@ -89,18 +98,27 @@ int gpulda_batch_loglik(void* handle, double* ll, uint64_t* skipped);
 int gpulda_batch_get_shapes(void* handle, GpuldaBatchShape* shapes);
 int gpulda_batch_set_shapes(void* handle, const GpuldaBatchShape* shapes);
 
+/* Selects the merged or per-bucket mode (GPULDA_BATCH_*) and, if
+ * merged_shape is not NULL, the merged launches' shape; takes effect at the
+ * next sweep. */
+int gpulda_batch_set_mode(void* handle, uint32_t mode, const GpuldaBatchShape* merged_shape);
+
 /* Autotuner.  For each bucket without an entry for this device in the cache
  * file, times the candidate shapes on the batch's own data (one Poisson draw
  * and one z sweep per candidate, with the counts and topics restored
  * afterwards, so the chains are unaffected), keeps the fastest and adds it to
- * the cache; buckets with an entry take it from the cache.  The cache is a
- * JSON object "<device>|sm<count>|K<=<bound>" -> [z_warps_per_block,
- * z_blocks_per_sm, phi_cells_per_block]; NULL cache_path tunes without one.
- * n_tuned (optional) receives how many buckets were timed. */
+ * the cache; buckets with an entry take it from the cache.  Then, unless the
+ * cache holds an entry for this batch's composition, it tunes the merged
+ * launches' shape the same way, times one whole iteration in each mode and
+ * keeps the faster mode.  The cache is a JSON object
+ * "<device>|sm<count>|K<=<bound>" -> [z_warps_per_block, z_blocks_per_sm,
+ * phi_cells_per_block] plus "<device>|sm<count>|merged|<bounds>N~<Mi tokens>"
+ * -> [the merged shape, merged mode 0/1]; NULL cache_path tunes without one.
+ * n_tuned (optional) receives how many entries were timed. */
 int gpulda_batch_tune(void* handle, const char* cache_path, uint32_t* n_tuned);
 
 /* Sizes: [0] problems, [1] tokens, [2] documents, [3] words, [4] cells,
- * [5] device bytes held, [6] buckets in use, [7] iterations run.
+ * [5] device bytes held, [6] buckets in use, [7] iterations run, [8] mode.
  * Returns the number of entries written (<= n). */
 int gpulda_batch_info(void* handle, uint64_t* out, int n);
 

@@ -17,7 +17,7 @@ import os
 
 import numpy as np
 
-from .build import LIB, build_oracle
+from .build import LIB, build_oracle, build_oracle_native
 
 _U32P = C.POINTER(C.c_uint32)
 _U64P = C.POINTER(C.c_uint64)
@@ -28,14 +28,25 @@ STREAM_INIT, STREAM_PHI, STREAM_Z = 1, 2, 3
 POIS_N, POIS_W, LFAC_N = 64, 192, 256
 
 _lib = None
+_path = LIB
+
+
+def use_native_build() -> str:
+    """Switches this process to the -march=native build of the oracle (built
+    here if needed; same results bit for bit).  For the timed CPU baseline;
+    call before any other use of the oracle."""
+    global _path
+    assert _lib is None, "the oracle is already loaded"
+    _path = build_oracle_native()
+    return _path
 
 
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
+        if _path == LIB and not os.path.exists(LIB):
             build_oracle()
-        L = C.CDLL(LIB)
+        L = C.CDLL(_path)
         L.orc_philox.argtypes = [_U32P, C.c_uint32, C.c_uint32, C.c_uint32, _U32P]
         L.orc_tables.argtypes = [C.c_float, _U32P, _U8P, _F64P]
         L.orc_poisson.argtypes = [_U32P, _U64P, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32, C.c_uint32,

@@ -1,9 +1,10 @@
-"""Batched chains (include/gpulda_batch.h) against solo runs: every problem
-of a batch -- K buckets of 64, 256, 1024 and 2048 topics side by side, two
-problems sharing a bucket -- must give the topics and counts of its solo
-Sampler run with the same seed and chain bit for bit, and the same joint
-log-likelihood within 1e-4 relative, through graph replays, a change of launch
-shapes, and an autotuning pass (which must leave the chains untouched)."""
+"""Batched chains (include/gpulda_batch.h) against the CPU oracle and solo
+runs: every problem of a batch -- K buckets of 64, 256, 1024 and 2048 topics
+side by side, two problems sharing a bucket -- must give the topics and counts
+of the oracle's chain (and of its solo Sampler run) with the same seed and
+chain bit for bit, and the same joint log-likelihood within 1e-4 relative,
+through graph replays, a change of launch shapes, and an autotuning pass
+(which must leave the chains untouched)."""
 import dataclasses
 import json
 
@@ -79,21 +80,53 @@ def test_batch_equals_solo(specs, solo):
         assert abs(ll1[p] - solo[p][2][0]) <= 1e-4 * abs(solo[p][2][0])
 
 
+def test_batch_equals_oracle_chains(specs, oracle_lib):
+    """Each problem's chain in the batch against oracle.Chain directly: the
+    initial counts, then topics, counts and log-likelihood after each of
+    three iterations (reference semantics src/cu/polyaurn.cu:61-123,
+    src/cu/topics.cu:36-105)."""
+    chains = [oracle_lib.Chain(sp.K, sp.alpha, sp.beta, sp.counts, seed=sp.seed, chain=sp.chain) for sp in specs]
+    zs = [sp.z.copy() for sp in specs]
+    with BatchChains(specs) as b:
+        for p, ch in enumerate(chains):
+            assert (b.counts(p) == ch.n).all(), f"problem {p}: initial counts differ from the oracle"
+        for it in range(3):
+            b.sweep(1)
+            ll, _ = b.loglik()
+            for p, (sp, ch) in enumerate(zip(specs, chains)):
+                ch.sample_phi()
+                r = ch.sweep(sp.w, zs[p], sp.d_len, want_ll=True)
+                assert (b.z(p) == zs[p]).all(), f"iteration {it}, problem {p}: topics differ from the oracle"
+                assert (b.counts(p) == ch.n).all(), f"iteration {it}, problem {p}: counts differ from the oracle"
+                assert abs(ll[p] - r["ll"]) <= 1e-4 * abs(r["ll"]), (it, p, ll[p], r["ll"])
+
+
 def test_batch_shapes_and_autotuner_leave_chains_unchanged(specs, solo, tmp_path):
     cache = tmp_path / "tune.json"
     with BatchChains(specs) as b:
+        assert b.info()["merged"] == 1  # one launch per stage over every problem by default
         b.sweep(1)
         n_tuned = b.tune(str(cache))
-        assert n_tuned == 4
+        assert n_tuned == 5  # four buckets and the merged launches
         entries = json.loads(cache.read_text())
-        assert len(entries) == 4 and all(len(v) == 3 for v in entries.values())
+        bucket_keys = [k for k in entries if "|K<=" in k]
+        merged_keys = [k for k in entries if "|merged|" in k]
+        assert len(bucket_keys) == 4 and all(len(entries[k]) == 3 for k in bucket_keys)
+        assert len(merged_keys) == 1 and len(entries[merged_keys[0]]) == 4
         b.sweep(1)
+        # per-bucket mode with other shapes, then merged mode with another shape
         b.set_shapes([(2, 0, 4096), (4, 4, 16384), (8, 2, 100000), (2, 0, 7)])
-        b.sweep(2)
+        b.set_mode(False)
+        assert b.info()["merged"] == 0
+        b.sweep(1)
+        b.set_mode(True, (4, 2, 50000))
+        b.sweep(1)
         _check(b, specs, solo, 3)
     with BatchChains(specs) as b:
-        assert b.tune(str(cache)) == 0  # every bucket from the cache
-        assert [list(s) for s in b.shapes()] == [entries[k] for k in sorted(entries, key=lambda k: int(k.split("<=")[1]))]
+        assert b.tune(str(cache)) == 0  # every entry from the cache
+        assert [list(s) for s in b.shapes()] == [entries[k] for k in sorted(bucket_keys,
+                                                                           key=lambda k: int(k.split("<=")[1]))]
+        assert b.info()["merged"] == entries[merged_keys[0]][3]
 
 
 def test_batch_async_on_caller_stream(specs, solo):

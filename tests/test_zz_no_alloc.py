@@ -64,3 +64,47 @@ def test_noalloc_sweep_matches_buffer_entry_point(gpu_lib):
                                               c.n_tokens, None)
         assert rc == g.GPULDA_ERR_UNSUPPORTED
         assert L.gpulda_last_error() == g.GPULDA_ERR_UNSUPPORTED
+
+
+def _large_k_corpus():
+    import dataclasses
+    wl = dataclasses.replace(corpus.WORKLOADS["large_k10000"], K=4096, V=3000, D=400)
+    return corpus.generate(wl, seed=6)
+
+
+@pytest.mark.parametrize("K", [20, 4096])
+def test_noalloc_on_caller_stream_without_host_sync(gpu_lib, K):
+    """Three iterations whose sweeps run on a stream of the caller's (a torch
+    stream, not the library's), with no host synchronization between a sweep
+    and the next sample_phi: the Phi step must wait for the sweep on the GPU.
+    At K=4096 the large-K store is used.  The chain must equal the buffer
+    entry point's, topics and counts bit for bit, log-likelihood within 1e-4
+    relative."""
+    c = corpus.generate("small", seed=3, D=300) if K == 20 else _large_k_corpus()
+    assert c.K == K
+    n_iter = 3
+    z = c.z.copy()
+    with g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=c.n_tokens, max_D=c.n_docs, seed=SEED,
+                   flags=g.GPULDA_FLAG_LOGLIK) as s:
+        for _ in range(n_iter):
+            s.sample_phi()
+            s.sweep_buffer(0, z, c.w, c.d_len, c.k_d())
+        n_want = s.read_state(q=False, alias=False, A=False, S=False, nnz=False)["n"]
+        ll_want = s.loglik()[0]
+    dz, dw, dd = _device_u32(c.z), _device_u32(c.w), _device_u32(c.d_len)
+    torch.cuda.synchronize()
+    st = torch.cuda.Stream()
+    L = g.lib()
+    with g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=c.n_tokens, max_D=c.n_docs, seed=SEED,
+                   flags=g.GPULDA_FLAG_LOGLIK) as s:
+        for _ in range(n_iter):
+            s.sample_phi()
+            rc = L.gpulda_sample_z_device_noalloc(dz.data_ptr(), dw.data_ptr(), dd.data_ptr(), c.n_docs,
+                                                  c.n_tokens, st.cuda_stream)
+            assert rc == g.GPULDA_OK
+        st.synchronize()
+        assert (dz.cpu().numpy().view(np.uint32) == z).all(), "topics differ from the buffer entry point"
+        n = s.read_state(q=False, alias=False, A=False, S=False, nnz=False)["n"]
+        assert (n == n_want).all(), "counts differ from the buffer entry point"
+        ll = s.loglik()[0]
+        assert abs(ll - ll_want) <= 1e-4 * abs(ll_want)
