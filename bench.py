@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     p.add_argument("--no-large", action="store_true", help="skip the large-K summary of the default line")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-chains summary of the default line")
+    p.add_argument("--warp-per-doc", action="store_true",
+                   help="sweep one document per warp (GPULDA_FLAG_WARP_PER_DOC) instead of two")
     p.add_argument("--large-steps", type=int, default=3, help="large-K summary: timed iterations")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU seconds per timed oracle iteration")
     p.add_argument("--problems", type=int, default=64, help="batched workload: number of problems")
@@ -317,7 +319,8 @@ def run_ours(args):
     hbm, peak_kind = peaks()
 
     # ---- device-resident corpus: value + roofline ----------------------------
-    s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=0, chain=rank)
+    zflags = g.GPULDA_FLAG_WARP_PER_DOC if args.warp_per_doc else 0
+    s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=0, chain=rank, flags=zflags)
     s.set_stream(stream.cuda_stream)
     s.corpus_load(c.z.copy(), c.w, c.d_len)
     for _ in range(args.warmup):
@@ -350,6 +353,8 @@ def run_ours(args):
         dist.barrier()
     s.set_stream(0)
     nnz_total = int(s.read_state(n=False, q=False, alias=False, A=False, S=False)["nnz"].astype(np.int64).sum())
+    # the standalone count rebuild over the same topics (leaves n as the last sweep rebuilt it)
+    rebuild_ms = float(np.median([s.corpus_count_rebuild() for _ in range(3)]))
 
     # ---- serving fold-in against the model just trained (one GPU) ----------
     serving = None
@@ -401,7 +406,7 @@ def run_ours(args):
     if not args.no_e2e:
         def protocol(zn, wn, dn, kn):
             s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=c.n_tokens, max_D=c.n_docs, seed=0,
-                          chain=rank)
+                          chain=rank, flags=zflags)
             for _ in range(args.warmup):
                 s.sample_phi()
                 s.sweep_buffer(0, zn, wn, dn, kn)
@@ -449,7 +454,11 @@ def run_ours(args):
                             "(list and alias entry); z sweep as in roofline (the count rebuild is its atomics)",
                     "phi_draw": 12 * c.K * c.V / (float(np.mean(draw_ms)) / 1e3) / 1e9,
                     "alias_build": (8 * c.K * c.V + 16 * nnz_total) / (float(np.mean(alias_ms)) / 1e3) / 1e9,
-                    "z_sweep": z_gbs},
+                    "z_sweep": z_gbs,
+                    "count_rebuild": 16 * c.n_tokens / (rebuild_ms / 1e3) / 1e9,
+                    "count_rebuild_note": "gpulda_corpus_count_rebuild over the corpus's topics after the timed "
+                                          "iterations: 16 B per token (read w and z, read-modify-write n), "
+                                          "warp-aggregated atomics; the sweep fuses the same rebuild"},
                 "sparse_work_per_token": float(np.mean(S_work)) / c.n_tokens,
                 "gpu_launches": launches, "clocks": clk, "e2e": e2e, "e2e_pageable": e2e_pageable,
                 "cpu_baseline": cpu, "serving": serving, "large_k10000": large, "batched": batched}

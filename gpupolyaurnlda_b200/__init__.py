@@ -28,6 +28,7 @@ GPULDA_ERR_DEVICE = 6
 GPULDA_ERR_UNSUPPORTED = 7
 GPULDA_FLAG_LOGLIK = 1
 GPULDA_FLAG_HASHMAP = 2
+GPULDA_FLAG_WARP_PER_DOC = 4
 GPULDA_MAX_K = 32768
 GPULDA_MAX_DOC_LEN = 65535
 POIS_TABLE_N, POIS_TABLE_W, LOGFAC_N = 64, 192, 256
@@ -132,6 +133,7 @@ _SIGNATURES = {
     "gpulda_corpus_load": (C.c_int, [_U32P, _U32P, _U32P, C.c_uint32, C.c_uint64]),
     "gpulda_corpus_sweep": (C.c_int, [C.c_uint32]),
     "gpulda_corpus_read_z": (C.c_int, [_U32P]),
+    "gpulda_corpus_count_rebuild": (C.c_int, [_F32P]),
     "gpulda_kernel_times": (C.c_int, [_F32P, C.c_int]),
     "gpulda_counters": (C.c_int, [_U64P, C.c_int]),
     "gpulda_debug_read": (C.c_int, [_U32P, _U32P, _U64P, _U64P, _U64P, _U32P]),
@@ -275,6 +277,13 @@ class Sampler:
 
     def corpus_sweep(self, n_iter: int = 1) -> None:
         check(self.L.gpulda_corpus_sweep(n_iter), "corpus_sweep")
+
+    def corpus_count_rebuild(self) -> float:
+        """Rebuilds the counts from the resident corpus's topics; returns the
+        kernel's device time in ms."""
+        ms = C.c_float()
+        check(self.L.gpulda_corpus_count_rebuild(C.byref(ms)), "corpus_count_rebuild")
+        return ms.value
 
     def corpus_z(self) -> np.ndarray:
         out = np.empty(len(self._corpus[0]), dtype=np.uint32)

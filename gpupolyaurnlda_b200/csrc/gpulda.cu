@@ -426,7 +426,8 @@ int z_launch(cudaStream_t s, u32* z, const u32* w, const u32* d_len, const u32* 
   zl.n_tokens = n_tokens;
   zl.tok_base = tok_base;
   zl.t = (u32)g.t;
-  zl.flags = (g.flags & GPULDA_FLAG_LOGLIK) ? 1u : 0u;
+  zl.flags = ((g.flags & GPULDA_FLAG_LOGLIK) ? kZFlagLoglik : 0u) |
+             ((g.flags & GPULDA_FLAG_WARP_PER_DOC) ? kZFlagWarpPerDoc : 0u);
   zl.counters = g.counters;
   zl.ll = g.ll;
   zl.work = work;
@@ -850,6 +851,20 @@ extern "C" int gpulda_corpus_sweep(uint32_t n_iter) {
   return check_status();
 }
 
+extern "C" int gpulda_corpus_count_rebuild(float* ms) {
+  if (!g.live || !g.cz) return fail(GPULDA_ERR_STATE, "corpus_count_rebuild without a loaded corpus");
+  cudaStream_t s = main_stream();
+  if (int rc = after_noalloc(s)) return rc;
+  CK(cudaMemsetAsync(g.dev.n, 0, (size_t)g.K * g.V * 4, s));
+  CK(cudaEventRecord(g.ev[4], s));
+  launch_count_rebuild(g.dev.n, g.cw, g.cz, g.c_tokens, g.K, g.V, g.status, s);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(g.ev[5], s));
+  CK(cudaStreamSynchronize(s));
+  if (ms) CK(cudaEventElapsedTime(ms, g.ev[4], g.ev[5]));
+  return check_status();
+}
+
 extern "C" int gpulda_corpus_read_z(uint32_t* z_out) {
   if (!g.live || !g.cz) return fail(GPULDA_ERR_STATE, "no corpus loaded");
   CK(cudaDeviceSynchronize());
@@ -1041,7 +1056,8 @@ extern "C" int gpulda_sample_z_device_noalloc(uint32_t* z, const uint32_t* w, co
   zl.n_tokens = n_tokens;
   zl.tok_base = g.tok_offset;
   zl.t = (u32)g.t;
-  zl.flags = (g.flags & GPULDA_FLAG_LOGLIK) ? 1u : 0u;
+  zl.flags = ((g.flags & GPULDA_FLAG_LOGLIK) ? kZFlagLoglik : 0u) |
+             ((g.flags & GPULDA_FLAG_WARP_PER_DOC) ? kZFlagWarpPerDoc : 0u);
   zl.counters = g.counters;
   zl.ll = g.ll;
   zl.work = work;

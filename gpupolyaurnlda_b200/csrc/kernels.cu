@@ -115,6 +115,41 @@ __global__ void __launch_bounds__(256, 4) phi_draw_kernel(ModelDev m, u32 t, u32
   }
 }
 
+// Phi draw for K a multiple of 4 (the common case): block (bx, by) draws rows
+// [bx * rows, (bx + 1) * rows) of topics [1024 by, 1024 (by + 1)); thread i
+// owns the four topics 1024 by + 4 i .. + 3 for every row of the block, so its
+// 16-byte loads and stores of consecutive threads are contiguous, and it keeps
+// the four per-topic sums in registers across the rows: the normalisers need
+// no shared memory and one 64-bit atomic per (block, topic) at the end.  Cell
+// c = w K + k uses word c & 3 of Philox block c >> 2, exactly as phi_rows, so
+// the draws are the same.
+__global__ void __launch_bounds__(256, 4) phi_draw_cols_kernel(ModelDev m, u32 t, u32 rows_per_block) {
+  const u32 K = m.K;
+  const u32 k0 = blockIdx.y * 1024u + 4u * threadIdx.x;
+  if (k0 >= K) return;
+  const u32 w0 = blockIdx.x * rows_per_block;
+  const u32 w1 = min(m.V, w0 + rows_per_block);
+  const double beta = (double)m.beta;
+  u64 acc[4] = {0, 0, 0, 0};
+  for (u32 w = w0; w < w1; ++w) {
+    const u64 cb = (u64)w * K + k0;
+    const U4 r = draw4(cb >> 2, t, kStreamPhi, 0, m.key0, m.key1);
+    const uint4 v = *reinterpret_cast<const uint4*>(m.n + cb);
+    const u32 nv[4] = {v.x, v.y, v.z, v.w};
+    u32 xv[4];
+#pragma unroll
+    for (u32 u = 0; u < 4; ++u) {
+      xv[u] = poisson_draw(nv[u], beta, u4_word(r, u), cb + u, t, kStreamPhi, m.key0, m.key1, m.tables);
+      acc[u] += xv[u];
+    }
+    *reinterpret_cast<uint4*>(m.q + cb) = make_uint4(xv[0], xv[1], xv[2], xv[3]);
+    *reinterpret_cast<uint4*>(m.n + cb) = make_uint4(0, 0, 0, 0);
+  }
+#pragma unroll
+  for (u32 u = 0; u < 4; ++u)
+    if (acc[u]) atomicAdd((unsigned long long*)&m.S[k0 + u], (unsigned long long)acc[u]);
+}
+
 // Batched Phi draw: block b draws rows [w0, w1) (problem-local word ids) of
 // problem p, with (p, w0, w1) from the block table.
 __global__ void __launch_bounds__(256) phi_draw_batch_kernel(ModelDev ar, BatchPhiDev bp, const u32* t_dev) {
@@ -343,6 +378,65 @@ __global__ void __launch_bounds__(1024) doc_offsets_kernel(const u32* __restrict
   }
 }
 
+// ---------------------------------------------------------------------------
+// Count rebuild n[w][z] += 1 over a token range (reference: the atomicAdd per
+// token at the end of sample_topics, src/cu/topics.cu:95).  Tokens are read
+// four at a time (16-byte loads of w and z); per load slot the warp groups
+// lanes whose tokens hit the same cell (__match_any_sync) and the group's
+// lowest lane adds the group's size: one atomic per distinct cell per warp
+// step instead of one per token.  Topics >= K and words >= V are reported
+// and counted modulo K / V, like the sweeps.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) count_rebuild_kernel(u32* __restrict__ n, const u32* __restrict__ w,
+                                                            const u32* __restrict__ z, u64 n_tokens, u32 K, u32 V,
+                                                            u32* status) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 groups = (n_tokens + 3) / 4;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  u32 st = 0;
+  // warp-uniform trip count: every lane of a warp takes the same number of steps
+  const u64 g0 = (u64)blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+  for (u64 gb = g0; gb < groups; gb += stride) {
+    const u64 gi = gb + lane;
+    u32 wv[4] = {0, 0, 0, 0}, zv[4] = {0, 0, 0, 0};
+    u32 nv = 0;  // tokens of this group
+    if (gi < groups) {
+      const u64 t0 = gi * 4;
+      nv = (u32)(n_tokens - t0 < 4 ? n_tokens - t0 : 4);
+      if (nv == 4) {
+        const uint4 a = *reinterpret_cast<const uint4*>(w + t0);
+        const uint4 b = *reinterpret_cast<const uint4*>(z + t0);
+        wv[0] = a.x, wv[1] = a.y, wv[2] = a.z, wv[3] = a.w;
+        zv[0] = b.x, zv[1] = b.y, zv[2] = b.z, zv[3] = b.w;
+      } else {
+        for (u32 u = 0; u < nv; ++u) {
+          wv[u] = w[t0 + u];
+          zv[u] = z[t0 + u];
+        }
+      }
+    }
+#pragma unroll
+    for (u32 u = 0; u < 4; ++u) {
+      const bool on = u < nv;
+      u32 wu = wv[u], zu = zv[u];
+      if (on && wu >= V) {
+        st |= kStatusBadWord;
+        wu %= V;
+      }
+      if (on && zu >= K) {
+        st |= kStatusBadTopic;
+        zu %= K;
+      }
+      // lanes without a token get distinct keys that match no cell
+      const u64 cell = on ? (u64)wu * K + zu : ~(u64)lane;
+      const u32 peers = __match_any_sync(kFullMask, cell);
+      if (on && lane == (u32)(__ffs(peers) - 1)) atomicAdd(n + cell, (u32)__popc(peers));
+    }
+  }
+  st = __reduce_or_sync(kFullMask, st);
+  if (lane == 0 && st) atomicOr(status, st);
+}
+
 __global__ void debug_philox_kernel(const u32* ctr, u32 n, u32 k0, u32 k1, u32* out) {
   const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -412,6 +506,14 @@ void launch_alias_build_batch(const ModelDev& ar, const BatchPhiDev& bp, u32 Kma
 void launch_bump(u32* t, cudaStream_t s) { bump_kernel<<<1, 1, 0, s>>>(t); }
 
 void launch_phi_draw(const ModelDev& m, u32 t, cudaStream_t s) {
+  if (m.K % 4 == 0) {
+    // rows per block: about 64 Ki cells per block, at least 8 rows
+    const u32 tiles = (m.K + 1023) / 1024;
+    const u32 rows = std::max<u32>(8u, 65536u / std::min<u32>(m.K, 1024u));
+    const dim3 grid((m.V + rows - 1) / rows, tiles);
+    phi_draw_cols_kernel<<<grid, 256, 0, s>>>(m, t, rows);
+    return;
+  }
   const u32 rows = std::max<u32>(1u, 65536u / m.K);
   const u32 blocks = (m.V + rows - 1) / rows;
   const int smem_sums = m.K <= 8192;
@@ -459,6 +561,14 @@ void launch_alias_build(const ModelDev& m, cudaStream_t s, void* scratch, size_t
   } else {
     alias_build_kernel<<<blocks, nt, smem, s>>>(m, nullptr, 0, items);
   }
+}
+
+void launch_count_rebuild(u32* n, const u32* w, const u32* z, u64 n_tokens, u32 K, u32 V, u32* status,
+                          cudaStream_t s) {
+  if (!n_tokens) return;
+  const u64 groups = (n_tokens + 3) / 4;
+  const u32 blocks = (u32)std::max<u64>(1, std::min<u64>((groups + 255) / 256, (u64)device_sm_count() * 8));
+  count_rebuild_kernel<<<blocks, 256, 0, s>>>(n, w, z, n_tokens, K, V, status);
 }
 
 void launch_doc_offsets(const u32* d_len, u32* d_idx, u32 n_docs, cudaStream_t s) {

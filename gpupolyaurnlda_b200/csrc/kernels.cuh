@@ -115,10 +115,22 @@ void launch_phi_draw(const ModelDev& m, u32 t, cudaStream_t s);
 // Per word: q from x and S, A, nnz and the alias table.
 void launch_alias_build(const ModelDev& m, cudaStream_t s, void* scratch, size_t scratch_bytes);
 size_t alias_build_scratch_bytes(u32 K);
+// n[w[i]][z[i]] += 1 for every token (warp-aggregated atomics); w and z
+// 16-byte aligned.
+void launch_count_rebuild(u32* n, const u32* w, const u32* z, u64 n_tokens, u32 K, u32 V, u32* status,
+                          cudaStream_t s);
 // d_idx = exclusive scan of d_len.
 void launch_doc_offsets(const u32* d_len, u32* d_idx, u32 n_docs, cudaStream_t s);
-// One sweep over a set of documents.
+// ZLaunch.flags bits.
+constexpr u32 kZFlagLoglik = 1u;       // accumulate the joint log-likelihood
+constexpr u32 kZFlagWarpPerDoc = 2u;   // one warp per document even where two fit
+
+// One sweep over a set of documents: two documents per warp for K <= 1024
+// (zsweep_half.cu), else (or with kZFlagWarpPerDoc) one warp per document.
 void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s);
+// The two-documents-per-warp sweep; returns false without launching above
+// 1024 topics.
+bool launch_z_sweep_half(const ModelDev& m, const ZLaunch& z, cudaStream_t s);
 // One sweep over documents of many problems (arenas + tables), with the given
 // warps per block and cap on blocks per SM (0: as many as fit).
 void launch_z_sweep_batch(const ModelDev& arenas, const BatchDev& b, u32 Kmax, const ZLaunch& z, cudaStream_t s,

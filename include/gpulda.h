@@ -135,6 +135,9 @@ typedef struct GpuldaExArgs {
 /* K > 2048: keep each document's counts in the order-preserving Robin Hood
  * hash map instead of the default sorted (topic, count) list (same results). */
 #define GPULDA_FLAG_HASHMAP 2u
+/* K <= 1024: sweep one document per warp instead of the default two per warp
+ * (same results; kept for comparison). */
+#define GPULDA_FLAG_WARP_PER_DOC 4u
 
 /* initialize() with an explicit seed, chain id and flags. Returns an error
  * code (never exits). */
@@ -161,6 +164,14 @@ int gpulda_corpus_load(const uint32_t* z, const uint32_t* w, const uint32_t* d_l
                        uint32_t n_docs, uint64_t n_tokens);
 int gpulda_corpus_sweep(uint32_t n_iter);
 int gpulda_corpus_read_z(uint32_t* z_out);
+/* Rebuilds the count table n from the resident corpus's current topics
+ * (n[w][z] = tokens of word w with topic z; warp-aggregated atomics), e.g. to
+ * resume a chain from saved topics instead of the initial counts of
+ * initialize.  The next sample_phi draws Phi from these counts.  ms
+ * (optional) receives the rebuild kernel's device time.  No counterpart in
+ * the reference, whose rebuild is the per-token atomicAdd of sample_topics
+ * (src/cu/topics.cu:95); the sweeps here rebuild n the same way as they go. */
+int gpulda_corpus_count_rebuild(float* ms);
 
 /* Per-kernel device times (ms) of the last iteration, in this order:
  * [0] Phi/Poisson draw, [1] normaliser prep, [2] alias build,
