@@ -36,6 +36,10 @@ constexpr u32 kHalfMaxDocLen = 65535u;          // 16-bit counts
 constexpr u32 kHalfDead = 4;                    // dead list entries tolerated before compaction
 constexpr u32 kHalfRegs = 8;                    // chunk elements kept in registers (lists <= 128)
 constexpr u32 kHalfWarps = 12;                  // warps per block (24 documents)
+// The word's nonzero list is walked while it is shorter than this many times
+// the document's topic list: its entries are read contiguously (few cache
+// lines per element), where the document side gathers q from across the row.
+constexpr u32 kWordSideFactor = 1;
 constexpr size_t kHalfSlotBytes = kHalfMaxK * 2 /* counts */ + kHalfMaxK * 2 /* list */ +
                                   kHalfMaxK / 8 /* in-list bitmap */ + 16 * 32 /* staged tokens */;
 static_assert(kHalfSlotBytes % 128 == 0, "slot size");
@@ -264,7 +268,7 @@ __global__ void __launch_bounds__(32 * kHalfWarps, 2) z_sweep_half_kernel(HalfAr
       if (act && cz == 1u) --nz;
       __syncwarp();
       // sparse mass over this lane's contiguous chunk of the shorter list
-      const bool word_side = nw < nl;
+      const bool word_side = nw < kWordSideFactor * nl;
       const u32 len = act ? (word_side ? nw : nl) : 0u;
       const u32 cper = (len + 15) >> 4;
       const u32 e0 = min(len, hl * cper), e1 = min(len, e0 + cper);
