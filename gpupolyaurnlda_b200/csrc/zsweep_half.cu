@@ -35,6 +35,7 @@ constexpr u32 kHalfMaxK = 1024;                 // topics per model of this kern
 constexpr u32 kHalfMaxDocLen = 65535u;          // 16-bit counts
 constexpr u32 kHalfDead = 4;                    // dead list entries tolerated before compaction
 constexpr u32 kHalfRegs = 8;                    // chunk elements kept in registers (lists <= 128)
+constexpr u32 kHalfBatch = 4;                   // further chunk elements loaded per unrolled batch
 constexpr u32 kHalfWarps = 12;                  // warps per block (24 documents)
 // The word's nonzero list is walked while it is shorter than this many times
 // the document's topic list: its entries are read contiguously (few cache
@@ -273,13 +274,15 @@ __global__ void __launch_bounds__(32 * kHalfWarps, 2) z_sweep_half_kernel(HalfAr
       const u32 cper = (len + 15) >> 4;
       const u32 e0 = min(len, hl * cper), e1 = min(len, e0 + cper);
       const u32 n_my = e1 - e0;
-      const bool inr = cper <= kHalfRegs;
+      // The first kHalfRegs elements of the chunk keep their masses in
+      // registers; the rest are summed in unrolled batches of independent
+      // loads (a scalar loop would wait on each gather in turn).
       u32 kk[kHalfRegs], qq[kHalfRegs];
       u64 ms[kHalfRegs];
 #pragma unroll
       for (u32 c = 0; c < kHalfRegs; ++c) {
         u32 kx = 0, qx = 0;
-        if (inr && c < n_my) {
+        if (c < n_my) {
           if (word_side) {
             const u64 ent = __ldg(crow + e0 + c);
             kx = (u32)ent & 0xffffu;
@@ -293,35 +296,47 @@ __global__ void __launch_bounds__(32 * kHalfWarps, 2) z_sweep_half_kernel(HalfAr
       }
 #pragma unroll
       for (u32 c = 0; c < kHalfRegs; ++c)
-        if (inr && c < n_my && !word_side) qq[c] = __ldg(qrow + kk[c]);
-      u64 ls = 0;
+        if (c < n_my && !word_side) qq[c] = __ldg(qrow + kk[c]);
+      u64 first = 0;
 #pragma unroll
       for (u32 c = 0; c < kHalfRegs; ++c) {
         ms[c] = (u64)cnt[kk[c]] * qq[c];
-        ls += ms[c];
+        first += ms[c];
       }
-      if (!inr)
-        for (u32 e = e0; e < e1; ++e) {
-          u32 kx, qx;
-          if (word_side) {
-            const u64 ent = __ldg(crow + e);
-            kx = (u32)ent & 0xffffu;
-            qx = (u32)(ent >> 32);
-          } else {
-            kx = tl[e];
-            qx = __ldg(qrow + kx);
+      u64 ls = first;
+      for (u32 b = kHalfRegs; b < n_my; b += kHalfBatch) {
+        u32 kb[kHalfBatch], qb[kHalfBatch];
+#pragma unroll
+        for (u32 c = 0; c < kHalfBatch; ++c) {
+          u32 kx = 0, qx = 0;
+          if (b + c < n_my) {
+            if (word_side) {
+              const u64 ent = __ldg(crow + e0 + b + c);
+              kx = (u32)ent & 0xffffu;
+              qx = (u32)(ent >> 32);
+            } else {
+              kx = tl[e0 + b + c];
+            }
           }
-          ls += (u64)cnt[kx] * qx;
+          kb[c] = kx;
+          qb[c] = qx;
         }
+#pragma unroll
+        for (u32 c = 0; c < kHalfBatch; ++c)
+          if (b + c < n_my && !word_side) qb[c] = __ldg(qrow + kb[c]);
+#pragma unroll
+        for (u32 c = 0; c < kHalfBatch; ++c) ls += (u64)cnt[kb[c]] * qb[c];
+      }
       const u64 incl = half_incl_scan_u64(ls, hl);
       const u64 B = __shfl_sync(kFullMask, incl, 15, 16);
       int degenerate;
       const int sp = take_sparse(r0, alpha, Aw, B, &degenerate);
       const bool sparse = act && sp && !degenerate;
-      // sparse selection: lane f's chunk holds the crossing element
+      // sparse selection: lane f's chunk holds the crossing element; when it
+      // lies among lane f's register elements the topic is read from there
       const u64 target = scale_u32(r1, B);
       const u32 f = (__ffs(half_ballot(incl > target, hb)) - 1) & 15u;
-      u32 cx = kHalfRegs - 1, kc = kk[kHalfRegs - 1];
+      u32 kc = kk[kHalfRegs - 1];
       {
         u64 run = incl - ls;
         bool found = false;
@@ -330,19 +345,20 @@ __global__ void __launch_bounds__(32 * kHalfWarps, 2) z_sweep_half_kernel(HalfAr
           run += ms[c];
           if (!found && run > target) {
             found = true;
-            cx = c;
             kc = kk[c];
           }
         }
       }
       u32 k_sp = __shfl_sync(kFullMask, kc, f, 16);
-      // chunks beyond the registers: a second pass over lane f's chunk
-      const bool need2 = sparse && !inr;
+      const u64 pre_f = __shfl_sync(kFullMask, incl - ls, f, 16);
+      const u64 first_f = __shfl_sync(kFullMask, first, f, 16);
+      // otherwise a second pass over lane f's elements past its registers
+      const bool need2 = sparse && pre_f + first_f <= target;
       if (__any_sync(kFullMask, need2)) {
-        u64 run = __shfl_sync(kFullMask, incl - ls, f, 16);
+        u64 run = pre_f + first_f;
         const u32 f0 = min(len, f * cper), f1 = min(len, f0 + cper);
         bool found = !need2;
-        for (u32 s0e = f0; __any_sync(kFullMask, !found && s0e < f1); s0e += 16) {
+        for (u32 s0e = f0 + kHalfRegs; __any_sync(kFullMask, !found && s0e < f1); s0e += 16) {
           const u32 e = s0e + hl;
           const bool on = !found && e < f1;
           u64 mass = 0;
@@ -373,7 +389,6 @@ __global__ void __launch_bounds__(32 * kHalfWarps, 2) z_sweep_half_kernel(HalfAr
           }
         }
       }
-      (void)cx;
       // dense draw: lane j's alias entry and fourth word
       const u32 r3 = __shfl_sync(kFullMask, r.w, j, 16);
       const u64 ea = __shfl_sync(kFullMask, my_al, j, 16);
