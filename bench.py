@@ -59,8 +59,6 @@ def parse():
     p.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     p.add_argument("--no-large", action="store_true", help="skip the large-K summary of the default line")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-chains summary of the default line")
-    p.add_argument("--warp-per-doc", action="store_true",
-                   help="sweep one document per warp (GPULDA_FLAG_WARP_PER_DOC) instead of two")
     p.add_argument("--large-steps", type=int, default=3, help="large-K summary: timed iterations")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU seconds per timed oracle iteration")
     p.add_argument("--problems", type=int, default=64, help="batched workload: number of problems")
@@ -319,8 +317,7 @@ def run_ours(args):
     hbm, peak_kind = peaks()
 
     # ---- device-resident corpus: value + roofline ----------------------------
-    zflags = g.GPULDA_FLAG_WARP_PER_DOC if args.warp_per_doc else 0
-    s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=0, chain=rank, flags=zflags)
+    s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=0, chain=rank)
     s.set_stream(stream.cuda_stream)
     s.corpus_load(c.z.copy(), c.w, c.d_len)
     for _ in range(args.warmup):
@@ -406,7 +403,7 @@ def run_ours(args):
     if not args.no_e2e:
         def protocol(zn, wn, dn, kn):
             s = g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=c.n_tokens, max_D=c.n_docs, seed=0,
-                          chain=rank, flags=zflags)
+                          chain=rank)
             for _ in range(args.warmup):
                 s.sample_phi()
                 s.sweep_buffer(0, zn, wn, dn, kn)

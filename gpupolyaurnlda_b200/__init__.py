@@ -28,7 +28,6 @@ GPULDA_ERR_DEVICE = 6
 GPULDA_ERR_UNSUPPORTED = 7
 GPULDA_FLAG_LOGLIK = 1
 GPULDA_FLAG_HASHMAP = 2
-GPULDA_FLAG_WARP_PER_DOC = 4
 GPULDA_MAX_K = 32768
 GPULDA_MAX_DOC_LEN = 65535
 POIS_TABLE_N, POIS_TABLE_W, LOGFAC_N = 64, 192, 256

@@ -25,8 +25,7 @@ NVCC_FLAGS = ARCH + [
     "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
     "-Xptxas", "-v",
 ]
-LIB_SOURCES = ["gpulda.cu", "kernels.cu", "zsweep.cu", "zsweep_half.cu", "zsweep_map.cu", "batch.cu", "serve.cu",
-               "zsweep_pairs.cu"]
+LIB_SOURCES = ["gpulda.cu", "kernels.cu", "zsweep.cu", "zsweep_map.cu", "batch.cu", "serve.cu", "zsweep_pairs.cu"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:

@@ -426,8 +426,7 @@ int z_launch(cudaStream_t s, u32* z, const u32* w, const u32* d_len, const u32* 
   zl.n_tokens = n_tokens;
   zl.tok_base = tok_base;
   zl.t = (u32)g.t;
-  zl.flags = ((g.flags & GPULDA_FLAG_LOGLIK) ? kZFlagLoglik : 0u) |
-             ((g.flags & GPULDA_FLAG_WARP_PER_DOC) ? kZFlagWarpPerDoc : 0u);
+  zl.flags = (g.flags & GPULDA_FLAG_LOGLIK) ? kZFlagLoglik : 0u;
   zl.counters = g.counters;
   zl.ll = g.ll;
   zl.work = work;
@@ -1056,8 +1055,7 @@ extern "C" int gpulda_sample_z_device_noalloc(uint32_t* z, const uint32_t* w, co
   zl.n_tokens = n_tokens;
   zl.tok_base = g.tok_offset;
   zl.t = (u32)g.t;
-  zl.flags = ((g.flags & GPULDA_FLAG_LOGLIK) ? kZFlagLoglik : 0u) |
-             ((g.flags & GPULDA_FLAG_WARP_PER_DOC) ? kZFlagWarpPerDoc : 0u);
+  zl.flags = (g.flags & GPULDA_FLAG_LOGLIK) ? kZFlagLoglik : 0u;
   zl.counters = g.counters;
   zl.ll = g.ll;
   zl.work = work;

@@ -122,15 +122,10 @@ void launch_count_rebuild(u32* n, const u32* w, const u32* z, u64 n_tokens, u32 
 // d_idx = exclusive scan of d_len.
 void launch_doc_offsets(const u32* d_len, u32* d_idx, u32 n_docs, cudaStream_t s);
 // ZLaunch.flags bits.
-constexpr u32 kZFlagLoglik = 1u;       // accumulate the joint log-likelihood
-constexpr u32 kZFlagWarpPerDoc = 2u;   // one warp per document even where two fit
+constexpr u32 kZFlagLoglik = 1u;  // accumulate the joint log-likelihood
 
-// One sweep over a set of documents: two documents per warp for K <= 1024
-// (zsweep_half.cu), else (or with kZFlagWarpPerDoc) one warp per document.
+// One sweep over a set of documents.
 void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s);
-// The two-documents-per-warp sweep; returns false without launching above
-// 1024 topics.
-bool launch_z_sweep_half(const ModelDev& m, const ZLaunch& z, cudaStream_t s);
 // One sweep over documents of many problems (arenas + tables), with the given
 // warps per block and cap on blocks per SM (0: as many as fit).
 void launch_z_sweep_batch(const ModelDev& arenas, const BatchDev& b, u32 Kmax, const ZLaunch& z, cudaStream_t s,

@@ -221,7 +221,6 @@ void launch_impl(const ZKernelArgs& a, u32 n_docs, cudaStream_t s, u32 wpb, u32 
 
 void launch_z_sweep(const ModelDev& m, const ZLaunch& z, cudaStream_t s) {
   if (!z.n_docs) return;
-  if (!(z.flags & kZFlagWarpPerDoc) && launch_z_sweep_half(m, z, s)) return;
   ZKernelArgs a;
   a.m = m;
   a.z = z;

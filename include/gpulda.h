@@ -135,9 +135,6 @@ typedef struct GpuldaExArgs {
 /* K > 2048: keep each document's counts in the order-preserving Robin Hood
  * hash map instead of the default sorted (topic, count) list (same results). */
 #define GPULDA_FLAG_HASHMAP 2u
-/* K <= 1024: sweep one document per warp instead of the default two per warp
- * (same results; kept for comparison). */
-#define GPULDA_FLAG_WARP_PER_DOC 4u
 
 /* initialize() with an explicit seed, chain id and flags. Returns an error
  * code (never exits). */

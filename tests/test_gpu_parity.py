@@ -303,55 +303,6 @@ def test_mid_slice_teacher_forced(gpu_lib, oracle_lib, K):
             assert (np.bincount(c.w.astype(np.int64) * c.K + z_gpu, minlength=c.K * c.V) == n).all()
 
 
-@pytest.mark.parametrize("K", [20, 1000])
-def test_two_documents_per_warp_equals_oracle_and_warp_per_document(gpu_lib, oracle_lib, K):
-    """The default sweep for K <= 1024 keeps two documents per warp
-    (csrc/zsweep_half.cu); GPULDA_FLAG_WARP_PER_DOC selects one warp per
-    document (csrc/zsweep.cu).  Both must give the oracle's chain bit for bit
-    (topics, counts, sparse-work counters) and its log-likelihood within 1e-4,
-    on documents of 1 to 5000 tokens (uneven pairs within a warp, empty and
-    single-token documents included)."""
-    from gpupolyaurnlda_b200 import corpus
-    import dataclasses
-    if K == 20:
-        c = corpus.generate("small", seed=9, D=700)
-    else:
-        wl = dataclasses.replace(corpus.WORKLOADS["mid"], V=8000, D=3000)
-        c = corpus.generate(wl, seed=9, device="cuda")
-    # ragged: a few empty and single-token documents among the others
-    d = c.d_len.copy().astype(np.int64)
-    d[5] += d[6]
-    d[6] = 0
-    d[10] -= d[10] - 1
-    d[11] += c.d_len[10] - 1
-    d_len = d.astype(np.uint32)
-    assert d_len.sum() == c.n_tokens and (d_len == 0).any() and (d_len == 1).any()
-    runs = {}
-    for name, flags in (("half", 0), ("warp", g.GPULDA_FLAG_WARP_PER_DOC)):
-        with g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=11,
-                       flags=g.GPULDA_FLAG_LOGLIK | flags) as s:
-            s.corpus_load(c.z.copy(), c.w, d_len)
-            out = []
-            for _ in range(3):
-                s.corpus_sweep(1)
-                cnt = s.counters()
-                out.append((s.corpus_z(), s.read_state(q=False, alias=False, A=False, S=False, nnz=False)["n"],
-                            s.loglik()[0], cnt["sparse_work"], cnt["sparse_draws"], cnt["docs"], cnt["tokens"]))
-            runs[name] = out
-    ch = oracle_lib.Chain(c.K, c.alpha, c.beta, c.counts, seed=11)
-    z_orc = c.z.copy()
-    for it in range(3):
-        ch.sample_phi()
-        r = ch.sweep(c.w, z_orc, d_len, want_ll=True)
-        for name in runs:
-            z, n, ll, work, draws, docs, toks = runs[name][it]
-            assert (z == z_orc).all(), (name, it, int((z != z_orc).sum()))
-            assert (n == ch.n).all(), (name, it)
-            assert work == int(r["stats"][2]) and draws == int(r["stats"][3]), (name, it)
-            assert docs == len(d_len) and toks == c.n_tokens, (name, it)
-            assert abs(ll - r["ll"]) <= LL_RTOL * abs(r["ll"]), (name, it, ll, r["ll"])
-
-
 def test_count_rebuild_from_resident_topics(gpu_lib, oracle_lib, small_corpus):
     """gpulda_corpus_count_rebuild (warp-aggregated atomics) rebuilds exactly
     the counts the sweep rebuilt, n[w][z] = #tokens (reference: the per-token
