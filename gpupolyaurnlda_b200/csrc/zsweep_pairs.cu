@@ -135,15 +135,14 @@ __device__ __forceinline__ void pairs_add_at(u32* P, u32& nl, u32& nz, u32 pos, 
   ++nz;
 }
 
-// Three blocks per SM (68 registers, no spills).  LL: the launch accumulates
+// Four blocks per SM (64 registers, no spills).  LL: the launch accumulates
 // the joint log-likelihood (a separate instantiation, so the plain sweep keeps
 // no log-likelihood registers); the statistics are per-chunk sums in one
-// register, flushed to per-block shared counters.  Four blocks at 64 registers
-// also run without spills and win on a quarter of the K=10000 corpus
-// (D = 2e6: 117.6 vs 129.3 ms) but lose on the whole of it (D = 8e6: 787 vs
-// 482 ms), so three it is.
+// register, flushed to per-block shared counters.  At K=10000 the whole
+// sweep (long-document launch, then short-document launch) takes 446 ms over
+// 8e6 documents and 109 ms over 2e6, against 483 and 131 ms at three blocks.
 template <bool LL>
-__global__ void __launch_bounds__(256, 3) z_sweep_pairs_kernel(PairArgs a) {
+__global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
   extern __shared__ __align__(16) unsigned char zsm[];
   __shared__ unsigned long long blk_stats[4];  // tokens, documents, sparse work, sparse draws
   if (threadIdx.x < 4) blk_stats[threadIdx.x] = 0;
