@@ -72,6 +72,19 @@ __device__ __forceinline__ u32 pairs_lower_bound(const u32* P, u32 n, u32 k, u32
   return lo + __popc(__ballot_sync(kFullMask, lt));
 }
 
+// First index i in P[0..n) with topic(P[i]) >= k, by one lane's binary search.
+__device__ __forceinline__ u32 pairs_find(const u32* P, u32 n, u32 k) {
+  u32 lo = 0, hi = n;
+  while (lo < hi) {
+    const u32 mid = (lo + hi) >> 1;
+    if (topic_of(P[mid]) < k)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
 // Count of topic k in P[0..n) by one lane's binary search.
 __device__ __forceinline__ u32 pairs_count(const u32* P, u32 n, u32 k) {
   u32 lo = 0, hi = n;
@@ -115,13 +128,17 @@ __device__ __forceinline__ u32 pairs_compact(u32* P, u32 n, u32 lane) {
   return out;
 }
 
-// Count of topic k += 1 at its position; inserts it if absent.
+// Count of topic k += 1 at its position; inserts it if absent.  bm (may be
+// null): the bitmap of topics with a positive count, kept in step.
 __device__ __forceinline__ void pairs_add_at(u32* P, u32& nl, u32& nz, u32 pos, u32 k, u32 cap, u32 lane,
-                                             u32* status) {
+                                             u32* status, u32* bm) {
   const u32 e = pos < nl ? P[pos] : 0xffffffffu;
   __syncwarp();
   if (pos < nl && topic_of(e) == k) {
-    if (lane == 0) P[pos] = e + 1u;
+    if (lane == 0) {
+      P[pos] = e + 1u;
+      if (bm && count_of(e) == 0) bm[k >> 5] |= 1u << (k & 31);
+    }
     if (count_of(e) == 0) ++nz;  // a dead entry revived
     __syncwarp();
     return;
@@ -131,8 +148,25 @@ __device__ __forceinline__ void pairs_add_at(u32* P, u32& nl, u32& nz, u32 pos, 
     return;
   }
   pairs_insert(P, nl, pos, (k << 16) | 1u, lane);
+  if (bm && lane == 0) bm[k >> 5] |= 1u << (k & 31);
+  __syncwarp();
   ++nl;
   ++nz;
+}
+
+// Launches whose documents are at most this long keep the topic bitmap.
+constexpr u32 kBitmapMaxLen = 1024;
+
+// Whether topic k has a positive count (always true without the bitmap: the
+// caller then searches).
+template <bool BM>
+__device__ __forceinline__ bool in_doc(const u32* bm, u32 k) {
+  return !BM || ((bm[k >> 5] >> (k & 31)) & 1u);
+}
+
+// Shared memory per warp: entries, staged token data, and the bitmap.
+__host__ __device__ __forceinline__ size_t pairs_warp_bytes(u32 cap, u32 K, bool bm) {
+  return (size_t)cap * 4 + kTokStageBytes + (bm ? ((((size_t)K + 31) / 32 * 4 + 15) & ~(size_t)15) : 0);
 }
 
 // Four blocks per SM (64 registers, no spills).  LL: the launch accumulates
@@ -141,7 +175,15 @@ __device__ __forceinline__ void pairs_add_at(u32* P, u32& nl, u32& nz, u32 pos, 
 // register, flushed to per-block shared counters.  At K=10000 the whole
 // sweep (long-document launch, then short-document launch) takes 446 ms over
 // 8e6 documents and 109 ms over 2e6, against 483 and 131 ms at three blocks.
-template <bool LL>
+//
+// BM (launches whose lists are short, lmax <= kBitmapMaxLen): each warp also
+// keeps a bitmap of the topics with a positive count.  The document's entries
+// are then built from it (bitmap of the tokens' topics, its set bits in order,
+// then one binary search and shared-memory atomic per token) instead of one
+// warp-cooperative insert per token, and a word-side walk skips the binary
+// search of every word topic absent from the document (most of them; a lane
+// slot where no lane's topic is present costs no search at all).
+template <bool LL, bool BM>
 __global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
   extern __shared__ __align__(16) unsigned char zsm[];
   __shared__ unsigned long long blk_stats[4];  // tokens, documents, sparse work, sparse draws
@@ -151,9 +193,11 @@ __global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
   const ZLaunch& p = a.z;
   const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const u32 K = m.K, V = m.V;
-  unsigned char* wsm = zsm + (size_t)warp * ((size_t)a.cap * 4 + kTokStageBytes);
+  const u32 bmw = (K + 31) >> 5;  // bitmap words
+  unsigned char* wsm = zsm + (size_t)warp * pairs_warp_bytes(a.cap, K, BM);
   u32* P = (u32*)wsm;
   uint4* stage = (uint4*)(wsm + (size_t)a.cap * 4);
+  u32* bm = BM ? (u32*)(wsm + (size_t)a.cap * 4 + kTokStageBytes) : nullptr;
   const bool want_ll = LL;
 
   double ll_acc = 0.0, ll_skip = 0.0;
@@ -177,13 +221,53 @@ __global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
     }
     // build the sorted entries of the document's topics
     u32 nl = 0, nz = 0;
-    for (u32 i = 0; i < L; ++i) {
-      u32 k = p.z[off + i];
-      if (k >= K) {
-        status |= kStatusBadTopic;
-        k %= K;
+    if (BM) {
+      for (u32 i = lane; i < bmw; i += 32) bm[i] = 0;
+      __syncwarp();
+      for (u32 i = lane; i < L; i += 32) {
+        u32 k = p.z[off + i];
+        if (k >= K) {
+          status |= kStatusBadTopic;
+          k %= K;
+        }
+        atomicOr(bm + (k >> 5), 1u << (k & 31));
       }
-      pairs_add_at(P, nl, nz, pairs_lower_bound(P, nl, k, lane), k, a.cap, lane, &status);
+      __syncwarp();
+      // the set bits in ascending order, 32 words per round
+      for (u32 b = 0; b < bmw; b += 32) {
+        const u32 wi = b + lane;
+        u32 bits = wi < bmw ? bm[wi] : 0u;
+        const u32 c = __popc(bits);
+        u32 x = c;
+#pragma unroll
+        for (u32 o = 1; o < 32; o <<= 1) {
+          const u32 y = __shfl_up_sync(kFullMask, x, o);
+          if (lane >= o) x += y;
+        }
+        u32 pos = nl + x - c;
+        while (bits) {
+          P[pos++] = (wi * 32 + (u32)(__ffs(bits) - 1)) << 16;
+          bits &= bits - 1;
+        }
+        nl += __shfl_sync(kFullMask, x, 31);
+      }
+      __syncwarp();
+      // counts: one binary search and shared-memory atomic per token
+      for (u32 i = lane; i < L; i += 32) {
+        const u32 k = p.z[off + i] % K;
+        atomicAdd(P + pairs_find(P, nl, k), 1u);
+      }
+      __syncwarp();
+      nz = nl;
+    } else {
+      for (u32 i = 0; i < L; ++i) {
+        u32 k = p.z[off + i];
+        if (k >= K) {
+          status |= kStatusBadTopic;
+          k %= K;
+        }
+        pairs_add_at(P, nl, nz, pairs_lower_bound(P, nl, k, lane), k, a.cap, lane, &status, nullptr);
+      }
     }
 
     for (u32 base = 0; base < L; base += 32) {
@@ -224,7 +308,10 @@ __global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
           const u32 e = pz < nl ? P[pz] : 0u;
           __syncwarp();
           if (pz < nl && topic_of(e) == zj && count_of(e) > 0) {
-            if (lane == 0) P[pz] = e - 1u;
+            if (lane == 0) {
+              P[pz] = e - 1u;
+              if (BM && count_of(e) == 1) bm[zj >> 5] &= ~(1u << (zj & 31));
+            }
             if (count_of(e) == 1) --nz;
           }
           __syncwarp();
@@ -247,7 +334,9 @@ __global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
 #pragma unroll
             for (u32 c = 0; c < kRegChunk; ++c) {
               const u64 ent = c < n_my ? __ldg(crow + e0 + c) : 0ull;
-              ms[c] = c < n_my ? (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32) : 0ull;
+              ms[c] = c < n_my && in_doc<BM>(bm, (u32)ent & 0xffffu)
+                          ? (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32)
+                          : 0ull;
             }
           } else {
             u32 es[kRegChunk], qs[kRegChunk];
@@ -263,7 +352,8 @@ __global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
         } else if (word_side) {
           for (u32 e = e0; e < e1; ++e) {
             const u64 ent = __ldg(crow + e);
-            ls += (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32);
+            if (in_doc<BM>(bm, (u32)ent & 0xffffu))
+              ls += (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32);
           }
         } else {
           for (u32 e = e0; e < e1; ++e) {
@@ -304,7 +394,8 @@ __global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
                 if (e < f1) {
                   if (word_side) {
                     const u64 ent = __ldg(crow + e);
-                    mass = (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32);
+                    if (in_doc<BM>(bm, (u32)ent & 0xffffu))
+                      mass = (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32);
                   } else {
                     const u32 en = P[e];
                     mass = (u64)count_of(en) * __ldg(qrow + topic_of(en));
@@ -333,7 +424,7 @@ __global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
         }
         const u32 nzm = nz;
         if (pos == 0xffffffffu) pos = pairs_lower_bound(P, nl, k, lane);
-        pairs_add_at(P, nl, nz, pos, k, a.cap, lane, &status);
+        pairs_add_at(P, nl, nz, pos, k, a.cap, lane, &status, bm);
         if (nl - nz > kPairsMaxDead) nl = pairs_compact(P, nl, lane);
         if (lane == 0) {
           atomicAdd(m.n + row + k, 1u);
@@ -405,13 +496,16 @@ bool launch_z_sweep_pairs(const ModelDev& m, const ZLaunch& z, cudaStream_t s, u
   a.cap = z_pairs_cap(m.K, lmax);
   a.lg_a = std::lgamma((double)m.alpha);
   a.lg_Ka = std::lgamma((double)m.K * (double)m.alpha);
-  const size_t per_warp = (size_t)a.cap * 4 + kTokStageBytes;
+  const bool bmap = lmax <= kBitmapMaxLen;
+  const size_t per_warp = pairs_warp_bytes(a.cap, m.K, bmap);
   constexpr size_t kBudget = 200 * 1024;
   u32 wpb = 8;
   while (wpb > 1 && per_warp * wpb > kBudget) --wpb;
   if (per_warp * wpb > kBudget) return false;
   const size_t smem = per_warp * wpb;
-  auto kern = ((z.flags & 1u) && z.ll) ? z_sweep_pairs_kernel<true> : z_sweep_pairs_kernel<false>;
+  const bool ll = (z.flags & 1u) && z.ll;
+  auto kern = bmap ? (ll ? z_sweep_pairs_kernel<true, true> : z_sweep_pairs_kernel<false, true>)
+                   : (ll ? z_sweep_pairs_kernel<true, false> : z_sweep_pairs_kernel<false, false>);
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBudget);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, smem);
