@@ -158,8 +158,12 @@ __device__ void fold_request(const FoldCommon& a, DocCounts& dc, uint4* stage, c
         const u64 Aw = ((u64)s1.w << 32) | s1.z;
         u32 nzm;
         bool sp;
-        const u32 k = token_step<4u>(dc, zj, r0, r1, r.w, my_al, j, m.q + row, m.csr + row, nw, Aw, alpha, lane, &nzm,
-                                 &sp);
+        // as in the training sweep: as few register slots as the walk needs
+        const u32 cper_j = ((nw < dc.nl ? nw : dc.nl) + 31) >> 5;
+        const u32 k = cper_j <= 2 ? token_step<2u>(dc, zj, r0, r1, r.w, my_al, j, m.q + row, m.csr + row, nw, Aw, alpha,
+                                                   lane, &nzm, &sp)
+                                  : token_step<4u>(dc, zj, r0, r1, r.w, my_al, j, m.q + row, m.csr + row, nw, Aw, alpha,
+                                                   lane, &nzm, &sp);
         if (lane == j) new_z = k;
         __syncwarp();
       }
