@@ -164,6 +164,122 @@ __device__ __forceinline__ bool in_doc(const u32* bm, u32 k) {
   return !BM || ((bm[k >> 5] >> (k & 31)) & 1u);
 }
 
+// One token's draw over the document's entries P[0..nl) (bm: the optional
+// topic bitmap) and the word's row: the walk of the shorter side split into
+// 32 contiguous chunks, chunks of at most R elements kept in registers.
+// Returns the topic; *pos_out receives its entry when the document-side walk
+// found it (else 0xffffffff).
+template <bool BM, u32 R>
+__device__ __forceinline__ u32 pairs_draw(const u32* P, u32 nl, const u32* bm, const u32* __restrict__ qrow,
+                                          const u64* __restrict__ crow, u32 nw, u64 Aw, float alpha, bool word_side,
+                                          u32 zj, u32 r0, u32 r1, u32 my_r3, u64 my_al, u32 j, u32 lane,
+                                          u32* pos_out, int* sp_out, int* degenerate_out) {
+  const u32 len = word_side ? nw : nl;
+  const u32 cper = (len + 31) >> 5;
+  const u32 e0 = min(len, lane * cper), e1 = min(len, e0 + cper);
+  const bool in_regs = cper <= R;
+  u64 ms[R];
+  u64 ls = 0;
+  if (in_regs) {
+    const u32 n_my = e1 - e0;
+    if (word_side) {
+#pragma unroll
+      for (u32 c = 0; c < R; ++c) {
+        const u64 ent = c < n_my ? __ldg(crow + e0 + c) : 0ull;
+        ms[c] = c < n_my && in_doc<BM>(bm, (u32)ent & 0xffffu)
+                    ? (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32)
+                    : 0ull;
+      }
+    } else {
+      u32 es[R], qs[R];
+#pragma unroll
+      for (u32 c = 0; c < R; ++c) es[c] = c < n_my ? P[e0 + c] : 0u;
+#pragma unroll
+      for (u32 c = 0; c < R; ++c) qs[c] = c < n_my ? __ldg(qrow + topic_of(es[c])) : 0u;
+#pragma unroll
+      for (u32 c = 0; c < R; ++c) ms[c] = (u64)count_of(es[c]) * qs[c];
+    }
+#pragma unroll
+    for (u32 c = 0; c < R; ++c) ls += ms[c];
+  } else if (word_side) {
+    for (u32 e = e0; e < e1; ++e) {
+      const u64 ent = __ldg(crow + e);
+      if (in_doc<BM>(bm, (u32)ent & 0xffffu))
+        ls += (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32);
+    }
+  } else {
+    for (u32 e = e0; e < e1; ++e) {
+      const u32 en = P[e];
+      ls += (u64)count_of(en) * __ldg(qrow + topic_of(en));
+    }
+  }
+  const u64 incl = warp_incl_scan_u64(ls, lane);
+  const u64 B = __shfl_sync(kFullMask, incl, 31);
+  int degenerate;
+  const int sp = take_sparse(r0, alpha, Aw, B, &degenerate);
+  *sp_out = sp;
+  *degenerate_out = degenerate;
+  u32 k = zj;
+  u32 pos = 0xffffffffu;  // the new topic's entry, when the walk found it
+  if (!degenerate) {
+    if (sp) {
+      const u64 target = scale_u32(r1, B);
+      const u32 f = __ffs(__ballot_sync(kFullMask, incl > target)) - 1;
+      u32 ef;
+      if (in_regs) {
+        // lane f's first element whose inclusive prefix exceeds the target
+        u64 pre = incl - ls;
+        u32 cx = R - 1;
+#pragma unroll
+        for (u32 c = R - 1; c-- > 0;) {
+          u64 t = pre;
+#pragma unroll
+          for (u32 d = 0; d <= c; ++d) t += ms[d];
+          if (t > target) cx = c;
+        }
+        ef = f * cper + __shfl_sync(kFullMask, cx, f);
+      } else {
+        u64 run = __shfl_sync(kFullMask, incl - ls, f);
+        const u32 f0 = min(len, f * cper), f1 = min(len, f0 + cper);
+        ef = f1 - 1;
+        for (u32 s0 = f0; s0 < f1; s0 += 32) {
+          const u32 e = s0 + lane;
+          u64 mass = 0;
+          if (e < f1) {
+            if (word_side) {
+              const u64 ent = __ldg(crow + e);
+              if (in_doc<BM>(bm, (u32)ent & 0xffffu))
+                mass = (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32);
+            } else {
+              const u32 en = P[e];
+              mass = (u64)count_of(en) * __ldg(qrow + topic_of(en));
+            }
+          }
+          const u64 in2 = warp_incl_scan_u64(mass, lane);
+          const u64 tot = __shfl_sync(kFullMask, in2, 31);
+          if (run + tot > target) {
+            ef = s0 + __ffs(__ballot_sync(kFullMask, run + in2 > target)) - 1;
+            break;
+          }
+          run += tot;
+        }
+      }
+      if (word_side) {
+        k = (u32)__ldg(crow + ef) & 0xffffu;
+      } else {
+        k = topic_of(P[ef]);
+        pos = ef;
+      }
+    } else {
+      const u32 r3 = __shfl_sync(kFullMask, my_r3, j);
+      const u64 e = __shfl_sync(kFullMask, my_al, j);
+      k = alias_pick(e, r3);
+    }
+  }
+  *pos_out = pos;
+  return k;
+}
+
 // Shared memory per warp: entries, staged token data, and the bitmap.
 __host__ __device__ __forceinline__ size_t pairs_warp_bytes(u32 cap, u32 K, bool bm) {
   return (size_t)cap * 4 + kTokStageBytes + (bm ? ((((size_t)K + 31) / 32 * 4 + 15) & ~(size_t)15) : 0);
@@ -321,107 +437,15 @@ __global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
         // large K), so the word side is taken up to 4x the document's length
         // (measured best at K=10000 among 1x, 2x, 4x, 8x).
         const bool word_side = nw < 4 * nl;
-        const u32 len = word_side ? nw : nl;
-        const u32 cper = (len + 31) >> 5;
-        const u32 e0 = min(len, lane * cper), e1 = min(len, e0 + cper);
-        constexpr u32 kRegChunk = 4;
-        const bool in_regs = cper <= kRegChunk;
-        u64 ms[kRegChunk];
-        u64 ls = 0;
-        if (in_regs) {
-          const u32 n_my = e1 - e0;
-          if (word_side) {
-#pragma unroll
-            for (u32 c = 0; c < kRegChunk; ++c) {
-              const u64 ent = c < n_my ? __ldg(crow + e0 + c) : 0ull;
-              ms[c] = c < n_my && in_doc<BM>(bm, (u32)ent & 0xffffu)
-                          ? (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32)
-                          : 0ull;
-            }
-          } else {
-            u32 es[kRegChunk], qs[kRegChunk];
-#pragma unroll
-            for (u32 c = 0; c < kRegChunk; ++c) es[c] = c < n_my ? P[e0 + c] : 0u;
-#pragma unroll
-            for (u32 c = 0; c < kRegChunk; ++c) qs[c] = c < n_my ? __ldg(qrow + topic_of(es[c])) : 0u;
-#pragma unroll
-            for (u32 c = 0; c < kRegChunk; ++c) ms[c] = (u64)count_of(es[c]) * qs[c];
-          }
-#pragma unroll
-          for (u32 c = 0; c < kRegChunk; ++c) ls += ms[c];
-        } else if (word_side) {
-          for (u32 e = e0; e < e1; ++e) {
-            const u64 ent = __ldg(crow + e);
-            if (in_doc<BM>(bm, (u32)ent & 0xffffu))
-              ls += (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32);
-          }
-        } else {
-          for (u32 e = e0; e < e1; ++e) {
-            const u32 en = P[e];
-            ls += (u64)count_of(en) * __ldg(qrow + topic_of(en));
-          }
-        }
-        const u64 incl = warp_incl_scan_u64(ls, lane);
-        const u64 B = __shfl_sync(kFullMask, incl, 31);
-        int degenerate;
-        const int sp = take_sparse(r0, m.alpha, Aw, B, &degenerate);
-        u32 k = zj;
-        u32 pos = 0xffffffffu;  // the new topic's entry, when the walk found it
-        if (!degenerate) {
-          if (sp) {
-            const u64 target = scale_u32(r1, B);
-            const u32 f = __ffs(__ballot_sync(kFullMask, incl > target)) - 1;
-            u32 ef;
-            if (in_regs) {
-              // lane f's first element whose inclusive prefix exceeds the target
-              u64 pre = incl - ls;
-              u32 cx = kRegChunk - 1;
-#pragma unroll
-              for (u32 c = kRegChunk - 1; c-- > 0;) {
-                u64 t = pre;
-#pragma unroll
-                for (u32 d = 0; d <= c; ++d) t += ms[d];
-                if (t > target) cx = c;
-              }
-              ef = f * cper + __shfl_sync(kFullMask, cx, f);
-            } else {
-              u64 run = __shfl_sync(kFullMask, incl - ls, f);
-              const u32 f0 = min(len, f * cper), f1 = min(len, f0 + cper);
-              ef = f1 - 1;
-              for (u32 s0 = f0; s0 < f1; s0 += 32) {
-                const u32 e = s0 + lane;
-                u64 mass = 0;
-                if (e < f1) {
-                  if (word_side) {
-                    const u64 ent = __ldg(crow + e);
-                    if (in_doc<BM>(bm, (u32)ent & 0xffffu))
-                      mass = (u64)pairs_count(P, nl, (u32)ent & 0xffffu) * (u32)(ent >> 32);
-                  } else {
-                    const u32 en = P[e];
-                    mass = (u64)count_of(en) * __ldg(qrow + topic_of(en));
-                  }
-                }
-                const u64 in2 = warp_incl_scan_u64(mass, lane);
-                const u64 tot = __shfl_sync(kFullMask, in2, 31);
-                if (run + tot > target) {
-                  ef = s0 + __ffs(__ballot_sync(kFullMask, run + in2 > target)) - 1;
-                  break;
-                }
-                run += tot;
-              }
-            }
-            if (word_side) {
-              k = (u32)__ldg(crow + ef) & 0xffffu;
-            } else {
-              k = topic_of(P[ef]);
-              pos = ef;
-            }
-          } else {
-            const u32 r3 = __shfl_sync(kFullMask, r.w, j);
-            const u64 e = __shfl_sync(kFullMask, my_al, j);
-            k = alias_pick(e, r3);
-          }
-        }
+        // as few register slots as the walk's chunks need (lists of up to 64
+        // elements: 2)
+        const u32 cper_j = ((word_side ? nw : nl) + 31) >> 5;
+        u32 pos;
+        int sp, degenerate;
+        u32 k = cper_j <= 2 ? pairs_draw<BM, 2>(P, nl, bm, qrow, crow, nw, Aw, m.alpha, word_side, zj, r0, r1, r.w, my_al,
+                                                 j, lane, &pos, &sp, &degenerate)
+                            : pairs_draw<BM, 4>(P, nl, bm, qrow, crow, nw, Aw, m.alpha, word_side, zj, r0, r1, r.w, my_al,
+                                                 j, lane, &pos, &sp, &degenerate);
         const u32 nzm = nz;
         if (pos == 0xffffffffu) pos = pairs_lower_bound(P, nl, k, lane);
         pairs_add_at(P, nl, nz, pos, k, a.cap, lane, &status, bm);
