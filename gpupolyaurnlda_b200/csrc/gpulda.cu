@@ -100,9 +100,16 @@ constexpr u32 kShortDoc = 256;
 
 // Longest-first order with the short documents (length <= kShortDoc) first:
 // returns their count and the longest length among the rest.
+// Documents longer than kShortDoc and at most kMidDoc tokens are swept by a
+// launch of their own, sized for them (and with the large-K store's topic
+// bitmap); the few longer ones by another.
+constexpr u32 kMidDoc = 1024;
+
 struct DocSplit {
   u32 n_short = 0;
   u32 lmax_long = 0;
+  u32 n_huge = 0;    // documents longer than kMidDoc (the first of the long ones)
+  u32 lmax_mid = 0;  // longest document of at most kMidDoc tokens among the long ones
 };
 
 DocSplit split_longest_first(const u32* d_len, u32 n, std::vector<u32>& order, u32 K) {
@@ -117,6 +124,8 @@ DocSplit split_longest_first(const u32* d_len, u32 n, std::vector<u32>& order, u
     }
   sp.n_short = n - first_short;
   sp.lmax_long = first_short > 0 ? d_len[order[0]] : 0;
+  while (sp.n_huge < first_short && d_len[order[sp.n_huge]] > kMidDoc) ++sp.n_huge;
+  sp.lmax_mid = sp.n_huge < first_short ? d_len[order[sp.n_huge]] : 0;
   std::rotate(order.begin(), order.begin() + first_short, order.end());
   return sp;
 }
@@ -446,14 +455,19 @@ int z_step_async(cudaStream_t s, u32* z, const u32* w, const u32* d_len, u32* d_
   CK(cudaEventRecord(ev[1], s));
   int rc = GPULDA_OK;
   if (split && g.K > kMapMinK) {
-    // Long documents, then short ones, one launch each on `s`.  Run
+    // Documents over kMidDoc tokens, then those over kShortDoc, then the
+    // short ones, one launch each on `s`, each sized for its longest.  Run
     // concurrently on two streams the launches competed for whole SMs (each
     // fills the register file at four blocks per SM): at K=10000 over 8e6
     // documents the sweep took 489 ms concurrently with three blocks per SM,
     // 778 ms with four, and 446 ms one after the other with four.
-    if (n_docs > split->n_short)
-      rc = z_launch(s, z, w, d_len, d_idx, order + split->n_short, K_d, n_docs - split->n_short, n_tokens,
-                    g.tok_offset, work, split->lmax_long);
+    const u32 n_long = n_docs - split->n_short;
+    if (split->n_huge)
+      rc = z_launch(s, z, w, d_len, d_idx, order + split->n_short, K_d, split->n_huge, n_tokens, g.tok_offset, work,
+                    split->lmax_long);
+    if (!rc && n_long > split->n_huge)
+      rc = z_launch(s, z, w, d_len, d_idx, order + split->n_short + split->n_huge, K_d, n_long - split->n_huge,
+                    n_tokens, g.tok_offset, work + 1, split->lmax_mid);
     if (!rc && split->n_short)
       rc = z_launch(s, z, w, d_len, d_idx, order, K_d, split->n_short, n_tokens, g.tok_offset,
                     work + 1 + kPieces, kShortDoc);

@@ -23,11 +23,16 @@ def _workload(K, V, D, lens=("lognormal", 4.2, 0.6, 5, 2000)):
 STORES = [0, g.GPULDA_FLAG_HASHMAP]
 
 
+# (K, V, D, document lengths): the last case has documents of every launch
+# tier -- at most 256 tokens, up to 1024, and longer
 @pytest.mark.parametrize("store", STORES, ids=["pairs", "hashmap"])
-@pytest.mark.parametrize("K,V,D", [(4096, 3000, 3000), (10000, 2000, 1500)])
-def test_map_sweep_matches_oracle(gpu_lib, oracle_lib, K, V, D, store):
-    c = corpus.generate(_workload(K, V, D), seed=5, device="cuda")
+@pytest.mark.parametrize("K,V,D,lens", [(4096, 3000, 3000, None), (10000, 2000, 1500, None),
+                                        (4096, 2500, 500, ("lognormal", 6.0, 0.8, 5, 3000))])
+def test_map_sweep_matches_oracle(gpu_lib, oracle_lib, K, V, D, lens, store):
+    c = corpus.generate(_workload(K, V, D, **({"lens": lens} if lens else {})), seed=5, device="cuda")
     assert c.d_len.max() > 256 and c.d_len.min() <= 256  # both launches run
+    if lens:
+        assert c.d_len.max() > 1024 and ((c.d_len > 256) & (c.d_len <= 1024)).any()
     ch = oracle_lib.Chain(c.K, c.alpha, c.beta, c.counts, seed=3)
     z_orc = c.z.copy()
     with g.Sampler(c.alpha, c.beta, c.K, c.counts, buffer_size=16, max_D=4, seed=3,
