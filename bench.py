@@ -528,6 +528,11 @@ def batched_problems(args, device, chain: int):
     return specs
 
 
+BATCH_MODES = {0: "per-bucket concurrent branches",
+               1: "merged: one launch per stage over every problem",
+               2: "merged sweep: per-bucket Phi-step branches, one z sweep over every problem's documents"}
+
+
 def batched_measure(args, local: int, world: int, rank: int) -> dict:
     """Batched chains: all problems in one graph-replayed iteration (after the
     autotuner), against the same problems run one after another as solo
@@ -600,8 +605,7 @@ def batched_measure(args, local: int, world: int, rank: int) -> dict:
                         f"D in [1k,100k] x{args.batch_scale}, doc lengths lognormal(4.5,1.0); "
                         f"N={N} tokens, D={D} documents",
             "N": N, "D": D, "cells": info["cells"], "device_bytes": info["device_bytes"],
-            "mode": "merged: one launch per stage over every problem" if info.get("merged") else
-                    "per-bucket concurrent branches",
+            "mode": BATCH_MODES.get(info.get("mode"), "?"),
             "sequential": {"value": seq_value, "unit": UNIT, "ms_per_step": seq_max / args.steps,
                            "what": "the same problems one after another as solo models (gpulda_corpus_sweep), "
                                    "device time summed"},
@@ -611,7 +615,8 @@ def batched_measure(args, local: int, world: int, rank: int) -> dict:
                           "shapes": {b_: list(sh) for b_, sh in zip(("K<=64", "K<=256", "K<=1024", "K<=2048"),
                                                                      shapes) if sh[0]}},
             "setup_seconds": {"generate": t_gen, "create": t_create},
-            "gpu_launches": args.steps * (1 + (3 if info.get("merged") else 3 * info["buckets"])), "clocks": clk}
+            "gpu_launches": args.steps * (1 + {1: 3, 2: 2 * info["buckets"] + 1}.get(info.get("mode"), 3 * info["buckets"])),
+            "clocks": clk}
 
 
 def run_batched(args):

@@ -111,13 +111,13 @@ class BatchChains:
             arr[i] = BatchShape(a, b, c, 0)
         check(lib().gpulda_batch_set_shapes(self.h, arr), "batch set_shapes")
 
-    def set_mode(self, merged: bool, shape: tuple[int, int, int] | None = None) -> None:
-        """Merged mode (one launch per stage over every problem) or per-bucket
-        mode; `shape` sets the merged launches' (z warps per block, z blocks
-        per SM, Poisson cells per block)."""
+    def set_mode(self, mode: int, shape: tuple[int, int, int] | None = None) -> None:
+        """BATCH_PER_BUCKET, BATCH_MERGED (one launch per stage over every
+        problem) or BATCH_MERGED_SWEEP (per-bucket Phi step, one z sweep over
+        every problem); `shape` sets the merged launches' (z warps per block,
+        z blocks per SM, Poisson cells per block)."""
         sh = BatchShape(shape[0], shape[1], shape[2], 0) if shape else None
-        check(lib().gpulda_batch_set_mode(self.h, 1 if merged else 0, C.byref(sh) if sh else None),
-              "batch set_mode")
+        check(lib().gpulda_batch_set_mode(self.h, mode, C.byref(sh) if sh else None), "batch set_mode")
 
     def tune(self, cache_path: str | None = None) -> int:
         n = C.c_uint32(0)
@@ -128,8 +128,10 @@ class BatchChains:
     def info(self) -> dict:
         out = (C.c_uint64 * 9)()
         m = lib().gpulda_batch_info(self.h, out, 9)
-        keys = ("problems", "tokens", "docs", "words", "cells", "device_bytes", "buckets", "iterations", "merged")
+        keys = ("problems", "tokens", "docs", "words", "cells", "device_bytes", "buckets", "iterations", "mode")
         return {k: int(out[i]) for i, k in enumerate(keys[:m])}
 
 
-__all__ = ["BatchChains", "ProblemSpec", "GpuldaError"]
+BATCH_PER_BUCKET, BATCH_MERGED, BATCH_MERGED_SWEEP = 0, 1, 2
+
+__all__ = ["BatchChains", "ProblemSpec", "GpuldaError", "BATCH_PER_BUCKET", "BATCH_MERGED", "BATCH_MERGED_SWEEP"]

@@ -10,16 +10,19 @@
 // so that a bucket's cells, words, documents and tokens are contiguous.  The
 // iteration graph is
 //   bump t; zero S, log-likelihood sums, counters and work counters;
-//   merged mode (the default): one launch per stage over every problem --
+//   merged mode: one launch per stage over every problem --
 //     phi_draw_batch over all problems' rows, alias_build_batch over all
 //     words, and one z_sweep_kernel<BATCH> whose persistent warps take
 //     (problem, document) items longest first from one work queue spanning
 //     all buckets, shared memory sized for the largest K;
+//   merged-sweep mode (the default): each bucket's phi_draw_batch ->
+//     alias_build_batch as concurrent branches, then the one persistent z
+//     sweep of the merged mode;
 //   per-bucket mode: per bucket, as concurrent branches,
 //     phi_draw_batch -> alias_build_batch -> z_sweep_kernel<BATCH>;
 // and every kernel reads t from device memory, so the graph is captured once
 // and replayed for every iteration.  The autotuner picks launch shapes per
-// bucket and for the merged launches, and the faster mode.
+// bucket and for the merged launches, and the fastest mode.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -111,8 +114,10 @@ struct Batch {
   std::vector<Slot> slots;
   std::vector<u32> slot_of;  // user index -> slot
   Bucket bk[GPULDA_BATCH_BUCKETS];
-  // merged mode: one launch per stage over every problem
-  bool merged = true;
+  // GPULDA_BATCH_*: per-bucket branches, one launch per stage over every
+  // problem, or per-bucket Phi/alias branches and one z sweep over every
+  // problem's documents
+  u32 mode = GPULDA_BATCH_MERGED_SWEEP;
   GpuldaBatchShape mshape{8, 0, 65536, 0};
   u32 Kmax_all = 0;
   bool want_ll_all = false;
@@ -273,6 +278,24 @@ void merged_iteration(const Batch& b, cudaStream_t s) {
                        b.mshape.z_blocks_per_sm);
 }
 
+// Each bucket's Phi draw and alias build as concurrent branches (their own
+// block sizes and threads per word), then one z sweep over every problem's
+// documents on s.
+void merged_sweep_iteration(const Batch& b, cudaStream_t s) {
+  cudaEventRecord(b.fork, s);
+  for (u32 j = 0; j < GPULDA_BATCH_BUCKETS; ++j) {
+    const Bucket& bu = b.bk[j];
+    if (!bu.used) continue;
+    cudaStreamWaitEvent(bu.s, b.fork, 0);
+    launch_phi_draw_batch(b.ar, b.phidev(bu.block0), bu.n_blocks, bu.Kmax, b.t_dev, bu.s);
+    launch_alias_build_batch(b.ar, b.phidev(bu.block0), bu.Kmax, bu.word0, bu.word1, bu.s);
+    cudaEventRecord(bu.join, bu.s);
+    cudaStreamWaitEvent(s, bu.join, 0);
+  }
+  launch_z_sweep_batch(b.ar, b.zdev(), b.Kmax_all, z_args_merged(b, b.counters, b.ll), s, b.mshape.z_warps_per_block,
+                       b.mshape.z_blocks_per_sm);
+}
+
 // The bucket's three kernels on stream s (work counter zeroed by the caller).
 void bucket_iteration(const Batch& b, u32 j, cudaStream_t s) {
   const Bucket& bu = b.bk[j];
@@ -291,8 +314,10 @@ int capture_graph(Batch& b) {
   cudaMemsetAsync(b.ll, 0, (size_t)b.P * 16, s);
   cudaMemsetAsync(b.counters, 0, kCtrN * 8, s);
   cudaMemsetAsync(b.work, 0, (GPULDA_BATCH_BUCKETS + 1) * 4, s);
-  if (b.merged) {
+  if (b.mode == GPULDA_BATCH_MERGED) {
     merged_iteration(b, s);
+  } else if (b.mode == GPULDA_BATCH_MERGED_SWEEP) {
+    merged_sweep_iteration(b, s);
   } else {
     cudaEventRecord(b.fork, s);
     for (u32 j = 0; j < GPULDA_BATCH_BUCKETS; ++j) {
@@ -736,7 +761,7 @@ int tune_bucket(Batch& b, u32 j) {
 }
 
 // Tunes the merged launches' shape on the batch's own data, then times one
-// whole iteration in each mode and keeps the faster.  All counts and topics
+// whole iteration in each of the three modes and keeps the fastest.  All counts and topics
 // are saved first and restored at the end, and the iteration counter is put
 // back, so the chains are unaffected.
 int tune_merged(Batch& b) {
@@ -753,9 +778,9 @@ int tune_merged(Batch& b) {
   cudaEventCreate(&e1);
   const u32 t_next = (u32)(b.t + 1), t_cur = (u32)b.t;
   const GpuldaBatchShape keep = b.mshape;
-  const bool keep_mode = b.merged;
+  const u32 keep_mode = b.mode;
   GpuldaBatchShape best = keep;
-  bool best_merged = keep_mode;
+  u32 best_mode = keep_mode;
   float best_phi = 1e30f, best_z = 1e30f;
   auto restore = [&]() -> int {
     BCK(cudaMemcpyAsync(b.ar.n, n_save, b.cells * 4, cudaMemcpyDeviceToDevice, s));
@@ -805,16 +830,18 @@ int tune_merged(Batch& b) {
     // one whole iteration in each mode, from the same state
     b.mshape = best;
     if ((rc = upload_block_tables(b))) return rc;
-    float mode_ms[2] = {1e30f, 1e30f};
-    for (int m = 0; m < 2; ++m) {
-      b.merged = m == 1;
+    float mode_ms[3] = {1e30f, 1e30f, 1e30f};
+    for (u32 m = 0; m < 3; ++m) {
+      b.mode = m;
       b.drop_graph();
       if ((rc = capture_graph(b))) return rc;
       if ((rc = restore())) return rc;
       BCK(cudaMemcpyAsync(b.t_dev, &t_cur, 4, cudaMemcpyHostToDevice, s));  // the graph bumps it to t + 1
       if ((rc = time_on(s, e0, e1, [&] { cudaGraphLaunch(b.exec, s); }, &mode_ms[m]))) return rc;
     }
-    best_merged = mode_ms[1] <= mode_ms[0];
+    best_mode = 0;
+    for (u32 m = 1; m < 3; ++m)
+      if (mode_ms[m] < mode_ms[best_mode]) best_mode = m;
     return GPULDA_OK;
   };
   rc = run();
@@ -826,7 +853,7 @@ int tune_merged(Batch& b) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b.mshape = rc ? keep : best;
-  b.merged = rc ? keep_mode : best_merged;
+  b.mode = rc ? keep_mode : best_mode;
   b.drop_graph();
   const int rc2 = upload_block_tables(b);
   if (rc) return rc;
@@ -935,7 +962,7 @@ extern "C" int gpulda_batch_set_shapes(void* handle, const GpuldaBatchShape* sha
 
 extern "C" int gpulda_batch_set_mode(void* handle, uint32_t mode, const GpuldaBatchShape* merged_shape) {
   Batch* b = as_batch(handle);
-  if (!b || mode > GPULDA_BATCH_MERGED) return report_error(GPULDA_ERR_ARGS, "bad batch set_mode arguments");
+  if (!b || mode > GPULDA_BATCH_MERGED_SWEEP) return report_error(GPULDA_ERR_ARGS, "bad batch set_mode arguments");
   if (merged_shape) {
     const GpuldaBatchShape& sh = *merged_shape;
     if ((sh.z_warps_per_block != 2 && sh.z_warps_per_block != 4 && sh.z_warps_per_block != 8) ||
@@ -943,7 +970,7 @@ extern "C" int gpulda_batch_set_mode(void* handle, uint32_t mode, const GpuldaBa
       return report_error(GPULDA_ERR_ARGS, "shape: z_warps_per_block must be 2, 4 or 8, phi cells positive");
   }
   BCK(cudaDeviceSynchronize());
-  b->merged = mode == GPULDA_BATCH_MERGED;
+  b->mode = mode;
   if (merged_shape) b->mshape = *merged_shape;
   b->drop_graph();
   return upload_block_tables(*b);
@@ -983,12 +1010,12 @@ extern "C" int gpulda_batch_tune(void* handle, const char* cache_path, uint32_t*
   if (it != cache.end() && it->second.size() >= 4 &&
       (it->second[0] == 2 || it->second[0] == 4 || it->second[0] == 8) && it->second[2] > 0) {
     b->mshape = GpuldaBatchShape{(u32)it->second[0], (u32)it->second[1], (u32)it->second[2], 0};
-    b->merged = it->second[3] != 0;
+    b->mode = it->second[3] <= GPULDA_BATCH_MERGED_SWEEP ? (u32)it->second[3] : GPULDA_BATCH_MERGED_SWEEP;
   } else {
     const int rc = tune_merged(*b);
     if (rc) return rc;
     cache[mkey] = {b->mshape.z_warps_per_block, b->mshape.z_blocks_per_sm, b->mshape.phi_cells_per_block,
-                   b->merged ? 1ul : 0ul};
+                   (unsigned long)b->mode};
     ++tuned;
     changed = true;
   }
@@ -1006,7 +1033,7 @@ extern "C" int gpulda_batch_info(void* handle, uint64_t* out, int n) {
   if (!b || !out) return 0;
   u32 used = 0;
   for (auto& bu : b->bk) used += bu.used;
-  const uint64_t v[9] = {b->P, b->N, b->D, b->Vtot, b->cells, b->bytes, used, b->iters, b->merged ? 1u : 0u};
+  const uint64_t v[9] = {b->P, b->N, b->D, b->Vtot, b->cells, b->bytes, used, b->iters, b->mode};
   const int m = n < 9 ? n : 9;
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

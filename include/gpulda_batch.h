@@ -14,13 +14,15 @@
  * tokens and documents live in shared device arenas, grouped by K bucket
  * (K <= 64, <= 256, <= 1024, <= 2048).  One iteration of every problem is
  * one CUDA graph, the iteration number read from device memory so the same
- * graph replays for every iteration.  In the merged mode (the default) the
- * graph holds one launch per stage for all problems: a Poisson draw over
- * every problem's rows, an alias build over every word, and one persistent
- * z sweep whose warps take (problem, document) items, longest first, from a
- * single work queue spanning all buckets.  In the per-bucket mode each bucket
- * runs Poisson draw -> alias build -> z sweep as a concurrent branch with its
- * own launch shapes.  Both modes give the same chains bit for bit.
+ * graph replays for every iteration.  In the merged mode the graph holds one
+ * launch per stage for all problems: a Poisson draw over every problem's
+ * rows, an alias build over every word, and one persistent z sweep whose
+ * warps take (problem, document) items, longest first, from a single work
+ * queue spanning all buckets.  In the merged-sweep mode (the default) each
+ * bucket runs its Poisson draw and alias build as a concurrent branch, and
+ * the same one persistent z sweep follows.  In the per-bucket mode each
+ * bucket runs Poisson draw -> alias build -> z sweep as a concurrent branch
+ * with its own launch shapes.  All modes give the same chains bit for bit.
  *
  * Handles are independent of each other and of the single-model state of
  * gpulda.h.  Calls on one handle come from one host thread.  Errors follow
@@ -60,6 +62,7 @@ typedef struct GpuldaProblem {
 /* Modes (gpulda_batch_set_mode). */
 #define GPULDA_BATCH_PER_BUCKET 0u
 #define GPULDA_BATCH_MERGED 1u
+#define GPULDA_BATCH_MERGED_SWEEP 2u
 
 /* Launch shapes of one K bucket, or of the merged launches. */
 typedef struct GpuldaBatchShape {
@@ -98,9 +101,9 @@ int gpulda_batch_loglik(void* handle, double* ll, uint64_t* skipped);
 int gpulda_batch_get_shapes(void* handle, GpuldaBatchShape* shapes);
 int gpulda_batch_set_shapes(void* handle, const GpuldaBatchShape* shapes);
 
-/* Selects the merged or per-bucket mode (GPULDA_BATCH_*) and, if
- * merged_shape is not NULL, the merged launches' shape; takes effect at the
- * next sweep. */
+/* Selects the mode (GPULDA_BATCH_*) and, if merged_shape is not NULL, the
+ * shape of the merged launches (the merged modes' z sweep, and the merged
+ * mode's Poisson draw); takes effect at the next sweep. */
 int gpulda_batch_set_mode(void* handle, uint32_t mode, const GpuldaBatchShape* merged_shape);
 
 /* Autotuner.  For each bucket without an entry for this device in the cache
@@ -109,11 +112,11 @@ int gpulda_batch_set_mode(void* handle, uint32_t mode, const GpuldaBatchShape* m
  * afterwards, so the chains are unaffected), keeps the fastest and adds it to
  * the cache; buckets with an entry take it from the cache.  Then, unless the
  * cache holds an entry for this batch's composition, it tunes the merged
- * launches' shape the same way, times one whole iteration in each mode and
- * keeps the faster mode.  The cache is a JSON object
+ * launches' shape the same way, times one whole iteration in each of the
+ * three modes and keeps the fastest.  The cache is a JSON object
  * "<device>|sm<count>|K<=<bound>" -> [z_warps_per_block, z_blocks_per_sm,
  * phi_cells_per_block] plus "<device>|sm<count>|merged|<bounds>N~<Mi tokens>"
- * -> [the merged shape, merged mode 0/1]; NULL cache_path tunes without one.
+ * -> [the merged shape, mode]; NULL cache_path tunes without one.
  * n_tuned (optional) receives how many entries were timed. */
 int gpulda_batch_tune(void* handle, const char* cache_path, uint32_t* n_tuned);
 

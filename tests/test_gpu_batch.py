@@ -13,7 +13,8 @@ import pytest
 
 import gpupolyaurnlda_b200 as g
 from gpupolyaurnlda_b200 import corpus
-from gpupolyaurnlda_b200.batch import BatchChains, ProblemSpec
+from gpupolyaurnlda_b200.batch import (BATCH_MERGED, BATCH_MERGED_SWEEP, BATCH_PER_BUCKET, BatchChains,
+                                       ProblemSpec)
 
 pytestmark = pytest.mark.gpu
 
@@ -104,7 +105,7 @@ def test_batch_equals_oracle_chains(specs, oracle_lib):
 def test_batch_shapes_and_autotuner_leave_chains_unchanged(specs, solo, tmp_path):
     cache = tmp_path / "tune.json"
     with BatchChains(specs) as b:
-        assert b.info()["merged"] == 1  # one launch per stage over every problem by default
+        assert b.info()["mode"] == BATCH_MERGED_SWEEP  # the default
         b.sweep(1)
         n_tuned = b.tune(str(cache))
         assert n_tuned == 5  # four buckets and the merged launches
@@ -113,20 +114,22 @@ def test_batch_shapes_and_autotuner_leave_chains_unchanged(specs, solo, tmp_path
         merged_keys = [k for k in entries if "|merged|" in k]
         assert len(bucket_keys) == 4 and all(len(entries[k]) == 3 for k in bucket_keys)
         assert len(merged_keys) == 1 and len(entries[merged_keys[0]]) == 4
-        b.sweep(1)
-        # per-bucket mode with other shapes, then merged mode with another shape
+        assert entries[merged_keys[0]][3] in (BATCH_PER_BUCKET, BATCH_MERGED, BATCH_MERGED_SWEEP)
+        # every mode, with other shapes: the chains must not change
         b.set_shapes([(2, 0, 4096), (4, 4, 16384), (8, 2, 100000), (2, 0, 7)])
-        b.set_mode(False)
-        assert b.info()["merged"] == 0
+        b.set_mode(BATCH_PER_BUCKET)
+        assert b.info()["mode"] == BATCH_PER_BUCKET
         b.sweep(1)
-        b.set_mode(True, (4, 2, 50000))
+        b.set_mode(BATCH_MERGED, (4, 2, 50000))
+        b.sweep(1)
+        b.set_mode(BATCH_MERGED_SWEEP, (2, 0, 65536))
         b.sweep(1)
         _check(b, specs, solo, 3)
     with BatchChains(specs) as b:
         assert b.tune(str(cache)) == 0  # every entry from the cache
         assert [list(s) for s in b.shapes()] == [entries[k] for k in sorted(bucket_keys,
                                                                            key=lambda k: int(k.split("<=")[1]))]
-        assert b.info()["merged"] == entries[merged_keys[0]][3]
+        assert b.info()["mode"] == entries[merged_keys[0]][3]
 
 
 def test_batch_async_on_caller_stream(specs, solo):
