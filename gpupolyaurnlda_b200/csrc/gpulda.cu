@@ -98,13 +98,14 @@ void longest_first(const u32* d_len, u32 n, std::vector<u32>& order) {
 constexpr u32 kMapMinK = 2048;
 constexpr u32 kShortDoc = 256;
 
-// Longest-first order with the short documents (length <= kShortDoc) first:
-// returns their count and the longest length among the rest.
 // Documents longer than kShortDoc and at most kMidDoc tokens are swept by a
 // launch of their own, sized for them (and with the large-K store's topic
 // bitmap); the few longer ones by another.
 constexpr u32 kMidDoc = 1024;
 
+// Longest-first order with the short documents (length <= kShortDoc) first:
+// their count, the longest length among the rest, and how many of the rest
+// are longer than kMidDoc (they come first among them).
 struct DocSplit {
   u32 n_short = 0;
   u32 lmax_long = 0;
