@@ -173,8 +173,8 @@ def roofline_profile(workload: str, c) -> dict:
     if c.K > 2048:
         return {"kernel": "z_sweep_pairs_kernel", "traffic": None,
                 "traffic_note": "the committed ncu capture of this kernel is a V=14,000 case "
-                                "(profiles/z_sweep_pairs_kernel_K10000_small_case.md: about 900 DRAM bytes per token "
-                                "at a 57 % L2 hit rate); its hit rate does not carry over to V=140,000, so no "
+                                "(profiles/z_sweep_pairs_kernel_K10000_small_case.md: about 1.2 kB of DRAM traffic per "
+                                "token at a 49 % L2 hit rate); its hit rate does not carry over to V=140,000, so no "
                                 "traffic is scaled to this launch"}
     out = {"kernel": "z_sweep_kernel",
            "binding_resource": "L1 data pipe (70 % of wavefront slots in the ncu profile), issue (64 %) and "
