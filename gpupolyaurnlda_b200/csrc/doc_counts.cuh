@@ -5,8 +5,8 @@
 // Reference: sample_topics / count_topics / compute_product_cumsum /
 // draw_wary_search / draw_alias, src/cu/topics.cu:36-105 and
 // src/cu/topics.cuh:63-192.  One warp owns one document.  Its counts m_d are
-// a dense array of 16-bit counts plus the sorted list of its nonzero topics
-// and an in-list bitmap.  Per token (after removing its current topic):
+// a dense array of 16-bit counts plus the sorted list of its nonzero topics.
+// Per token (after removing its current topic):
 //   B      = sum_k m_dk * q[w][k]      (u64, exact)
 //   sparse iff u0 * (alpha*A[w] + B) < B
 //   sparse: target = floor(u1 * B); topic = first k in ascending order whose
@@ -37,30 +37,33 @@ namespace gpulda {
 // 8 -> 36.8, 16 -> 37.2, 32 -> 38.2, 64 -> 39.3.
 constexpr u32 kMaxDead = 4;
 
-// Shared memory per warp for documents of up to Kmax topics: counts and list
-// (2 x Kp u16) and the in-list bitmap.
+// Shared memory per warp for documents of up to Kmax topics: the 16-bit
+// counts (Kmax rounded up to 32 entries: the list build scans them 32 at a
+// time) and the sorted list (at most Kmax distinct topics, rounded up to 8
+// entries).  Both parts are multiples of 16 bytes.  Every byte counts here:
+// shared memory comes out of the SM's 256 KB L1, and the q gathers of the
+// walk live on L1 hits (mid corpus: 1.6 KB more per warp took the carveout
+// from 196 to 228 KB, L1 from 60 to 28 KB, and the sweep from 2.72e9 to
+// 2.30e9 tokens/s).
 __host__ __device__ __forceinline__ size_t doc_counts_bytes(u32 Kmax) {
-  const size_t Kp = (Kmax + 63) & ~63u;
-  return Kp * 4 + ((Kp / 8 + 15) & ~(size_t)15);
+  return (size_t)((Kmax + 31) & ~31u) * 2 + (size_t)((Kmax + 7) & ~7u) * 2;
 }
 
 struct DocCounts {
-  uint16_t* cnt;  // dense counts, Kp entries
+  uint16_t* cnt;  // dense counts, Kmax rounded up to 32 entries
   // Sorted topics of the document: every topic with a nonzero count, plus
   // topics whose count fell to zero since the last compaction (their mass is
-  // zero, so they never change B or the selected topic).
+  // zero, so they never change B or the selected topic).  Entries are
+  // distinct topics, so the list never holds more than K.
   uint16_t* tl;
-  u32* inl;  // bitmap: topic is in tl
   u32 nz;    // topics with a nonzero count
   u32 nl;    // list length (nz plus dead entries)
 };
 
 __device__ __forceinline__ DocCounts doc_counts_at(unsigned char* base, u32 Kmax) {
-  const u32 Kpmax = (Kmax + 63) & ~63u;
   DocCounts dc;
   dc.cnt = (uint16_t*)base;
-  dc.tl = dc.cnt + Kpmax;
-  dc.inl = (u32*)(dc.tl + Kpmax);
+  dc.tl = dc.cnt + ((Kmax + 31) & ~31u);
   dc.nz = dc.nl = 0;
   return dc;
 }
@@ -82,9 +85,8 @@ __device__ __forceinline__ u32 list_lower_bound(const uint16_t* tl, u32 n, u32 k
 }
 
 // Drops the entries of topics whose count is zero from the list tl[0..n)
-// (stable, in place, warp-cooperative) and clears their in-list bits.
-// Returns the new length.
-__device__ __forceinline__ u32 list_compact(uint16_t* tl, u32 n, const uint16_t* cnt, u32* inl, u32 lane) {
+// (stable, in place, warp-cooperative).  Returns the new length.
+__device__ __forceinline__ u32 list_compact(uint16_t* tl, u32 n, const uint16_t* cnt, u32 lane) {
   u32 out = 0;
   for (u32 b = 0; b < n; b += 32) {
     const u32 e = b + lane;
@@ -93,7 +95,6 @@ __device__ __forceinline__ u32 list_compact(uint16_t* tl, u32 n, const uint16_t*
     const u32 ball = __ballot_sync(kFullMask, keep);
     __syncwarp();
     if (keep) tl[out + __popc(ball & ((1u << lane) - 1u))] = (uint16_t)k;
-    if (e < n && !keep) atomicAnd(inl + (k >> 5), ~(1u << (k & 31)));
     out += __popc(ball);
     __syncwarp();
   }
@@ -118,7 +119,7 @@ __device__ __forceinline__ void list_insert(uint16_t* tl, u32 n, u32 pos, u32 k,
 // A topic >= K is counted modulo K and reported in *status.
 __device__ __forceinline__ void doc_counts_build(DocCounts& dc, const u32* z, u32 L, u32 K, u32 lane, u32* status,
                                                  u32 bad_topic_bit) {
-  const u32 Kp = (K + 63) & ~63u;
+  const u32 Kp = (K + 31) & ~31u;
   for (u32 i = lane; i < Kp / 8; i += 32) reinterpret_cast<uint4*>(dc.cnt)[i] = make_uint4(0, 0, 0, 0);
   __syncwarp();
   for (u32 i = lane; i < L; i += 32) {
@@ -130,17 +131,16 @@ __device__ __forceinline__ void doc_counts_build(DocCounts& dc, const u32* z, u3
     atomicAdd(reinterpret_cast<u32*>(dc.cnt) + (k >> 1), 1u << ((k & 1) * 16));
   }
   __syncwarp();
-  // Sorted list and bitmap, 32 topics per round: lane l tests topic b + l
-  // (consecutive 16-bit loads, free of bank conflicts, where a contiguous
-  // range per lane would put the lanes' loads 64 bytes apart); the round's
-  // ballot is its bitmap word and gives each nonzero topic its list position.
+  // Sorted list, 32 topics per round: lane l tests topic b + l (consecutive
+  // 16-bit loads, free of bank conflicts, where a contiguous range per lane
+  // would put the lanes' loads 64 bytes apart); the round's ballot gives each
+  // nonzero topic its list position.
   const u32 below = (1u << lane) - 1u;
   u32 pos = 0;
   for (u32 b = 0; b < Kp; b += 32) {
     const bool nz = dc.cnt[b + lane] != 0;
     const u32 m = __ballot_sync(kFullMask, nz);
     if (nz) dc.tl[pos + __popc(m & below)] = (uint16_t)(b + lane);
-    if (lane == 0) dc.inl[b >> 5] = m;
     pos += __popc(m);
   }
   __syncwarp();
@@ -280,14 +280,15 @@ __device__ __forceinline__ u32 token_step(DocCounts& dc, u32 zj, u32 r0, u32 r1,
   if (lane == 0) cnt[k] = (uint16_t)(ck + 1u);
   if (ck == 0u) {
     ++dc.nz;
-    if (!((dc.inl[k >> 5] >> (k & 31)) & 1u)) {
-      list_insert(tl, dc.nl, list_lower_bound(tl, dc.nl, k, lane), k, lane);
-      if (lane == 0) atomicOr(dc.inl + (k >> 5), 1u << (k & 31));
-      __syncwarp();
+    // A topic back from zero may still be in the list as a dead entry; the
+    // search that finds the insert position tells.
+    const u32 pos = list_lower_bound(tl, dc.nl, k, lane);
+    if (pos == dc.nl || tl[pos] != k) {
+      list_insert(tl, dc.nl, pos, k, lane);
       ++dc.nl;
     }
   }
-  if (dc.nl - dc.nz > kMaxDead) dc.nl = list_compact(tl, dc.nl, cnt, dc.inl, lane);
+  if (dc.nl - dc.nz > kMaxDead) dc.nl = list_compact(tl, dc.nl, cnt, lane);
   return k;
 }
 
