@@ -177,8 +177,8 @@ def roofline_profile(workload: str, c) -> dict:
                                 "token at a 49 % L2 hit rate); its hit rate does not carry over to V=140,000, so no "
                                 "traffic is scaled to this launch"}
     out = {"kernel": "z_sweep_kernel",
-           "binding_resource": "L1 data pipe (70 % of wavefront slots in the ncu profile), issue (64 %) and "
-                               "gather latency; DRAM at 2.4 %: 94 % of the gathers hit L2"}
+           "binding_resource": "L1 data pipe (74 % of wavefront slots in the ncu profile), issue (66 %) and "
+                               "gather latency; DRAM at 2.6 %: 93 % of the gathers hit L2, half of them L1"}
     tpt = measured_traffic_per_token()
     if workload == "mid" and tpt:
         out.update(traffic=tpt * c.n_tokens, traffic_note="ncu dram bytes per token of a 3.4e7-token slice, scaled to N")
