@@ -243,6 +243,7 @@ void free_model() {
   dfree(g.dev.csr);
   dfree(g.dev.A);
   dfree(g.dev.S);
+  dfree(g.dev.Sinv);
   dfree(g.dev.nnz);
   dfree(g.C);
   dfree(g.cdf);
@@ -305,7 +306,8 @@ int init_impl(const Args* args, Buffer* buffers, u32 n_buffers, const GpuldaExAr
   for (auto& e : g.z_ev) CK(cudaEventCreate(&e));
   if ((rc = dalloc(&g.dev.n, cells)) || (rc = dalloc(&g.dev.q, cells)) || (rc = dalloc(&g.dev.al, cells)) ||
       (rc = dalloc(&g.dev.csr, cells)) ||
-      (rc = dalloc(&g.dev.A, g.V)) || (rc = dalloc(&g.dev.S, g.K)) || (rc = dalloc(&g.dev.nnz, g.V)) ||
+      (rc = dalloc(&g.dev.A, g.V)) || (rc = dalloc(&g.dev.S, g.K)) || (rc = dalloc(&g.dev.Sinv, g.K)) ||
+      (rc = dalloc(&g.dev.nnz, g.V)) ||
       (rc = dalloc(&g.C, g.V)) || (rc = dalloc(&g.cdf, (size_t)kPoisN * kPoisW)) ||
       (rc = dalloc(&g.guide, (size_t)kPoisN * 256)) || (rc = dalloc(&g.lfac, kLogFacN)) ||
       (rc = dalloc(&g.counters, kCtrN)) || (rc = dalloc(&g.ll, 2)) || (rc = dalloc(&g.work, 2 + kPieces)) ||
@@ -405,7 +407,7 @@ int phi_step_async(cudaStream_t s) {
   launch_alias_build(g.dev, s, g.alias_scratch, g.alias_scratch_bytes);
   CK(cudaGetLastError());
   CK(cudaEventRecord(g.ev[3], s));
-  g.launches += 2;
+  g.launches += 3;  // Poisson draw, topic reciprocals, alias build
   g.phi_timed = true;
   return GPULDA_OK;
 }

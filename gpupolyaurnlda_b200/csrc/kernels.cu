@@ -123,27 +123,55 @@ __global__ void __launch_bounds__(256, 4) phi_draw_kernel(ModelDev m, u32 t, u32
 // no shared memory and one 64-bit atomic per (block, topic) at the end.  Cell
 // c = w K + k uses word c & 3 of Philox block c >> 2, exactly as phi_rows, so
 // the draws are the same.
-__global__ void __launch_bounds__(256, 4) phi_draw_cols_kernel(ModelDev m, u32 t, u32 rows_per_block) {
+#ifndef GPULDA_PHI_ROWS_IN_FLIGHT
+#define GPULDA_PHI_ROWS_IN_FLIGHT 4
+#endif
+#ifndef GPULDA_PHI_ZERO_FAST
+#define GPULDA_PHI_ZERO_FAST 1
+#endif
+// Rows whose counts each thread loads before drawing any of them: the draw of
+// a row waits on its 16-byte load, so loads of several rows in flight hide
+// the memory latency one row at a time would expose.  With four rows the loop
+// needs about 120 registers (two 256-thread blocks per SM); at 64 registers it
+// spilled (mid corpus: 1.75 TB/s of its 12 B per cell against 1.51 TB/s with
+// one row at a time and four blocks per SM).
+constexpr u32 kPhiRowsInFlight = GPULDA_PHI_ROWS_IN_FLIGHT;
+
+__global__ void __launch_bounds__(256, 2) phi_draw_cols_kernel(ModelDev m, u32 t, u32 rows_per_block) {
   const u32 K = m.K;
   const u32 k0 = blockIdx.y * 1024u + 4u * threadIdx.x;
   if (k0 >= K) return;
   const u32 w0 = blockIdx.x * rows_per_block;
   const u32 w1 = min(m.V, w0 + rows_per_block);
   const double beta = (double)m.beta;
+  // Most cells hold no tokens, and for n = 0 the inversion returns 0 exactly
+  // when the cell's word is below the table's first CDF entry: that entry in
+  // a register answers those cells without the guide and CDF loads.
+  const u32 cdf00 = __ldg(m.tables.cdf);
   u64 acc[4] = {0, 0, 0, 0};
-  for (u32 w = w0; w < w1; ++w) {
-    const u64 cb = (u64)w * K + k0;
-    const U4 r = draw4(cb >> 2, t, kStreamPhi, 0, m.key0, m.key1);
-    const uint4 v = *reinterpret_cast<const uint4*>(m.n + cb);
-    const u32 nv[4] = {v.x, v.y, v.z, v.w};
-    u32 xv[4];
+  for (u32 wb = w0; wb < w1; wb += kPhiRowsInFlight) {
+    uint4 v[kPhiRowsInFlight];
 #pragma unroll
-    for (u32 u = 0; u < 4; ++u) {
-      xv[u] = poisson_draw(nv[u], beta, u4_word(r, u), cb + u, t, kStreamPhi, m.key0, m.key1, m.tables);
-      acc[u] += xv[u];
+    for (u32 i = 0; i < kPhiRowsInFlight; ++i)
+      v[i] = wb + i < w1 ? *reinterpret_cast<const uint4*>(m.n + (u64)(wb + i) * K + k0) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+    for (u32 i = 0; i < kPhiRowsInFlight; ++i) {
+      if (wb + i >= w1) break;
+      const u64 cb = (u64)(wb + i) * K + k0;
+      const U4 r = draw4(cb >> 2, t, kStreamPhi, 0, m.key0, m.key1);
+      const u32 nv[4] = {v[i].x, v[i].y, v[i].z, v[i].w};
+      u32 xv[4];
+#pragma unroll
+      for (u32 u = 0; u < 4; ++u) {
+        const u32 ru = u4_word(r, u);
+        xv[u] = (GPULDA_PHI_ZERO_FAST && nv[u] == 0 && ru < cdf00)
+                    ? 0u
+                    : poisson_draw(nv[u], beta, ru, cb + u, t, kStreamPhi, m.key0, m.key1, m.tables);
+        acc[u] += xv[u];
+      }
+      *reinterpret_cast<uint4*>(m.q + cb) = make_uint4(xv[0], xv[1], xv[2], xv[3]);
+      *reinterpret_cast<uint4*>(m.n + cb) = make_uint4(0, 0, 0, 0);
     }
-    *reinterpret_cast<uint4*>(m.q + cb) = make_uint4(xv[0], xv[1], xv[2], xv[3]);
-    *reinterpret_cast<uint4*>(m.n + cb) = make_uint4(0, 0, 0, 0);
   }
 #pragma unroll
   for (u32 u = 0; u < 4; ++u)
@@ -262,9 +290,10 @@ __device__ void alias_build_block(const u64* ent, u32 n, u64 A, u64* vals, uint1
 // word's nonzeros fit smem_items, else the block's slice of global scratch.
 constexpr u32 kPerThread = 8;
 
-__device__ __forceinline__ void alias_word(u32 K, u32* __restrict__ qrow, const u64* __restrict__ S, u64* alrow,
-                                           u64* csrrow, u64* A_out, u32* nnz_out, u64* s_vals, uint16_t* s_idx,
-                                           u32 smem_items, u64* g_vals, uint16_t* g_idx, u64* sh) {
+__device__ __forceinline__ void alias_word(u32 K, u32* __restrict__ qrow, const u64* __restrict__ S,
+                                           const u64* __restrict__ Sinv, u64* alrow, u64* csrrow, u64* A_out,
+                                           u32* nnz_out, u64* s_vals, uint16_t* s_idx, u32 smem_items, u64* g_vals,
+                                           uint16_t* g_idx, u64* sh) {
   u64 part = 0, nz = 0;
   const u32 tile = blockDim.x * kPerThread;
   for (u32 t0 = 0; t0 < K; t0 += tile) {
@@ -277,11 +306,24 @@ __device__ __forceinline__ void alias_word(u32 K, u32* __restrict__ qrow, const 
       u64 qq = 0;
       if (k < K) {
         const u32 x = qrow[k];
-        if (x) {
-          qq = (((u64)x) << 32) / S[k];
+        if (x) {  // a zero count is already a zero q
+          const u64 num = (u64)x << 32, sk = S[k];
+          if (Sinv) {
+            // floor(num / sk) from the reciprocal: the multiply-high is at
+            // most 2 below the quotient
+            qq = __umul64hi(num, Sinv[k]);
+            u64 r = num - qq * sk;
+            if (r >= sk) {
+              ++qq;
+              r -= sk;
+            }
+            if (r >= sk) ++qq;
+          } else {
+            qq = num / sk;
+          }
           if (qq > 0xffffffffULL) qq = 0xffffffffULL;
+          qrow[k] = (u32)qq;
         }
-        qrow[k] = (u32)qq;
       }
       qv[c] = (u32)qq;
       cnt += qq != 0;
@@ -318,8 +360,8 @@ __global__ void __launch_bounds__(256) alias_build_kernel(ModelDev m, unsigned c
   uint16_t* g_idx = gscratch ? (uint16_t*)(g_vals + K) : nullptr;
   for (u32 w = blockIdx.x; w < m.V; w += gridDim.x) {
     const size_t row = (size_t)w * K;
-    alias_word(K, m.q + row, m.S, m.al + row, m.csr + row, m.A + w, m.nnz + w, s_vals, s_idx, smem_items, g_vals,
-               g_idx, sh);
+    alias_word(K, m.q + row, m.S, m.Sinv, m.al + row, m.csr + row, m.A + w, m.nnz + w, s_vals, s_idx, smem_items,
+               g_vals, g_idx, sh);
   }
 }
 
@@ -333,8 +375,19 @@ __global__ void __launch_bounds__(256) alias_build_batch_kernel(ModelDev ar, Bat
   for (u32 w = w0 + blockIdx.x; w < w1; w += gridDim.x) {
     const u32 pb = bp.wpid[w], K = bp.K[pb];
     const size_t row = bp.row_off[w];
-    alias_word(K, ar.q + row, ar.S + bp.S_off[pb], ar.al + row, ar.csr + row, ar.A + w, ar.nnz + w, vals, idx, Kmax,
-               nullptr, nullptr, sh);
+    alias_word(K, ar.q + row, ar.S + bp.S_off[pb], nullptr, ar.al + row, ar.csr + row, ar.A + w, ar.nnz + w, vals,
+               idx, Kmax, nullptr, nullptr, sh);
+  }
+}
+
+// Reciprocals of the per-topic normalisers, inv[k] = floor((2^64 - 1) / S[k])
+// (0 for an empty topic): the alias build then divides by a multiply-high and
+// at most two corrections instead of a 64-bit division per nonzero cell.
+__global__ void topic_recip_kernel(const u64* __restrict__ S, u64* __restrict__ inv, u32 K) {
+  const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < K) {
+    const u64 sk = S[k];
+    inv[k] = sk ? ~0ull / sk : 0ull;
   }
 }
 
@@ -546,6 +599,7 @@ size_t alias_build_scratch_bytes(u32 K) {
 }
 
 void launch_alias_build(const ModelDev& m, cudaStream_t s, void* scratch, size_t scratch_bytes) {
+  if (m.Sinv) topic_recip_kernel<<<(m.K + 255) / 256, 256, 0, s>>>(m.S, m.Sinv, m.K);
   const u32 nt = alias_threads(m.K);
   const u32 items = std::min(m.K, kAliasSmemItems);
   const size_t smem = alias_scratch_item_bytes(items);

@@ -29,6 +29,7 @@ struct ModelDev {
   u64* csr;    // V*K per-word lists of (q << 32 | k) for q > 0, ascending k, nnz[w] used
   u64* A;      // V   dense mass per word
   u64* S;      // K   per-topic normalisers
+  u64* Sinv;   // K   floor((2^64 - 1) / S[k]), written by the alias build's launch (null: divide)
   u32* nnz;    // V   nonzero x per word
   PoisTables tables;
 };

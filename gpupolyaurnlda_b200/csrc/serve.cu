@@ -813,6 +813,7 @@ extern "C" int gpulda_serve_create_from_phi(const GpuldaServeArgs* args, uint32_
   if (e == cudaSuccess) {
     ModelDev md = s.fc.m;
     md.S = S;
+    md.Sinv = nullptr;  // a one-off build: plain divisions
     launch_alias_build(md, nullptr, scratch, sb);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
