@@ -146,7 +146,8 @@ __global__ void __launch_bounds__(256, 2) phi_draw_cols_kernel(ModelDev m, u32 t
   const double beta = (double)m.beta;
   // Most cells hold no tokens, and for n = 0 the inversion returns 0 exactly
   // when the cell's word is below the table's first CDF entry: that entry in
-  // a register answers those cells without the guide and CDF loads.
+  // a register answers those cells without the guide and CDF loads (K=10000:
+  // 4.06 against 3.86 TB/s; no difference at K=1000).
   const u32 cdf00 = __ldg(m.tables.cdf);
   u64 acc[4] = {0, 0, 0, 0};
   for (u32 wb = w0; wb < w1; wb += kPhiRowsInFlight) {
