@@ -439,14 +439,17 @@ __global__ void __launch_bounds__(256, 4) z_sweep_pairs_kernel(PairArgs a) {
         // topic bitmap, on 2e6 documents: 103 ms per sweep against 116 for
         // 2x, 115 for 8x and 126 for 16x).
         const bool word_side = nw < 4 * nl;
-        // as few register slots as the walk's chunks need (lists of up to 64
-        // elements: 2)
+        // as few register slots as the walk's chunks need: 2, 4 or 6 (K=10000,
+        // 2e6 documents: 101.8 ms per sweep against 102.9 with 2 or 4; an 8-slot
+        // path beside them spilled and took 108.4)
         const u32 cper_j = ((word_side ? nw : nl) + 31) >> 5;
         u32 pos;
         int sp, degenerate;
         u32 k = cper_j <= 2 ? pairs_draw<BM, 2>(P, nl, bm, qrow, crow, nw, Aw, m.alpha, word_side, zj, r0, r1, r.w, my_al,
                                                  j, lane, &pos, &sp, &degenerate)
-                            : pairs_draw<BM, 4>(P, nl, bm, qrow, crow, nw, Aw, m.alpha, word_side, zj, r0, r1, r.w, my_al,
+                : cper_j <= 4 ? pairs_draw<BM, 4>(P, nl, bm, qrow, crow, nw, Aw, m.alpha, word_side, zj, r0, r1, r.w, my_al,
+                                                 j, lane, &pos, &sp, &degenerate)
+                            : pairs_draw<BM, 6>(P, nl, bm, qrow, crow, nw, Aw, m.alpha, word_side, zj, r0, r1, r.w, my_al,
                                                  j, lane, &pos, &sp, &degenerate);
         const u32 nzm = nz;
         if (pos == 0xffffffffu) pos = pairs_lower_bound(P, nl, k, lane);
