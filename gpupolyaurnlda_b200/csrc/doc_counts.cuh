@@ -173,6 +173,8 @@ __device__ __forceinline__ u32 token_step(DocCounts& dc, u32 zj, u32 r0, u32 r1,
   if (cz == 1u) --dc.nz;  // the entry stays in the list until compaction
   __syncwarp();
   const u32 nl = dc.nl;
+  // the shorter list (mid corpus: taking the word's list up to 0.8x, 1.5x or 2x
+  // the document's gave 2.71e9, 2.72e9 and 2.68e9 tokens/s against 2.77e9)
   const bool word_side = nw < nl;
   // Sparse mass over this lane's contiguous chunk.
   const u32 len = word_side ? nw : nl;
