@@ -123,19 +123,13 @@ __global__ void __launch_bounds__(256, 4) phi_draw_kernel(ModelDev m, u32 t, u32
 // no shared memory and one 64-bit atomic per (block, topic) at the end.  Cell
 // c = w K + k uses word c & 3 of Philox block c >> 2, exactly as phi_rows, so
 // the draws are the same.
-#ifndef GPULDA_PHI_ROWS_IN_FLIGHT
-#define GPULDA_PHI_ROWS_IN_FLIGHT 4
-#endif
-#ifndef GPULDA_PHI_ZERO_FAST
-#define GPULDA_PHI_ZERO_FAST 1
-#endif
 // Rows whose counts each thread loads before drawing any of them: the draw of
 // a row waits on its 16-byte load, so loads of several rows in flight hide
 // the memory latency one row at a time would expose.  With four rows the loop
 // needs about 120 registers (two 256-thread blocks per SM); at 64 registers it
 // spilled (mid corpus: 1.75 TB/s of its 12 B per cell against 1.51 TB/s with
 // one row at a time and four blocks per SM).
-constexpr u32 kPhiRowsInFlight = GPULDA_PHI_ROWS_IN_FLIGHT;
+constexpr u32 kPhiRowsInFlight = 4;
 
 __global__ void __launch_bounds__(256, 2) phi_draw_cols_kernel(ModelDev m, u32 t, u32 rows_per_block) {
   const u32 K = m.K;
@@ -165,7 +159,7 @@ __global__ void __launch_bounds__(256, 2) phi_draw_cols_kernel(ModelDev m, u32 t
 #pragma unroll
       for (u32 u = 0; u < 4; ++u) {
         const u32 ru = u4_word(r, u);
-        xv[u] = (GPULDA_PHI_ZERO_FAST && nv[u] == 0 && ru < cdf00)
+        xv[u] = (nv[u] == 0 && ru < cdf00)
                     ? 0u
                     : poisson_draw(nv[u], beta, ru, cb + u, t, kStreamPhi, m.key0, m.key1, m.tables);
         acc[u] += xv[u];
